@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark: rays/s and ms/frame of the isosurface ray caster on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1] [--impl ours|reference]
+
+A step is one rendered frame of the workload:
+  c2 (default): the 2048^3 float32 out-of-core fly-through -- 256 seeded
+      anisotropic Gaussian blobs + 4-octave value noise, isovalue 0.6,
+      16^3 bricks (apron 3), device brick cache 4 GB, pinned host tier
+      16 GB, 1920x1080, orbit at radius 3000 voxels, 1.2 deg per frame.
+      Inputs exceed L2 (32 GB volume), no flush between frames.
+  c1: the 128^3 noisy sphere, fully resident in HBM, one 512x512 camera at
+      distance 300; L2 flushed (256 MB write) between timed frames.
+value = rays of all ranks / device time (CUDA events, max over ranks).
+Multi-GPU: replicas only -- each rank renders its own frames, no
+collective on the data path ("scaling": "weak").
+
+--impl reference times the reference algorithm's CPU restatement (the
+oracle port; the reference itself has no CPU path) on the host cores, on a
+bounded sample of the same workload; rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+
+CONFIGS = {
+    "c1": dict(workload="128^3 f32 noisy sphere (|x-c|+N(0,0.25)), iso 40, resident, 512x512, FOV 60 deg, "
+                        "distance 300, 8^3 bricks, 4^3 candidate nodes",
+               gen="sphere", seed=1234, n=128, iso=40.0, levelC=4, levelO=5, inc=3, W=512, H=512, fov=30.0,
+               dist=50.0, resident=1, l2flush=True, orbit=None, cam_pos=(63.5, 63.5, 363.5)),
+    "c2": dict(workload="2048^3 f32 blobs+noise, iso 0.6, out-of-core: 16^3 bricks (apron 3), 4 GB device "
+                        "cache, 16 GB pinned host tier, 1920x1080, orbit r=3000 at 1.2 deg/frame",
+               gen="blobs", seed=2048, n=2048, iso=0.6, levelC=7, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
+               dist=50.0, resident=0, l2flush=False, orbit=(3000.0, 1.2), dev_bytes=4 << 30,
+               host_bytes=16 << 30),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(", ") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) >= 9 for i in range(4) if "Active" in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- workload
+def orbit_camera(vt, cfg, frame):
+    """Pose on the orbit: position c + r (sin a, 0, cos a), looking at c, up +y,
+    right = cross(look, up) (the reference's basis convention)."""
+    r, step = cfg["orbit"]
+    c = (cfg["n"] - 1) / 2.0
+    a = math.radians(step * frame)
+    cam = vt.Camera(cfg["H"], cfg["W"], cfg["dist"], cfg["fov"], cfg["fov"]).c
+    pos = np.array([c + r * math.sin(a), c, c + r * math.cos(a)], np.float32)
+    look = (np.array([c, c, c], np.float32) - pos)
+    look = (look / np.sqrt(np.float32((look * look).sum()))).astype(np.float32)
+    up = np.array([0, 1, 0], np.float32)
+    right = np.cross(look, up).astype(np.float32)
+    for i in range(3):
+        cam.look[i], cam.up[i], cam.right[i], cam.position[i] = look[i], up[i], right[i], pos[i]
+    return cam
+
+
+def static_camera(vt, cfg):
+    cam = vt.Camera(cfg["H"], cfg["W"], cfg["dist"], cfg["fov"], cfg["fov"])
+    cam.Move(cfg["cam_pos"])
+    return cam.c
+
+
+def frame_camera(vt, cfg, frame):
+    return orbit_camera(vt, cfg, frame) if cfg["orbit"] else static_camera(vt, cfg)
+
+
+class Workload:
+    """Volume (device generated), octree (GPU builder) and renderer."""
+
+    def __init__(self, cfg, torch, device, workdir, need_renderer=True, host_copy=False):
+        import visualtur_b200 as vt
+        self.vt, self.cfg = vt, cfg
+        n = cfg["n"]
+        t0 = time.time()
+        dvol = torch.empty(n * n * n, dtype=torch.float32, device=device)
+        if cfg["gen"] == "sphere":
+            c = (n - 1) / 2.0
+            vt.generate_volume(vt.VT_GEN_SPHERE, cfg["seed"], (n, n, n), (c, c, c, 0.25), device_ptr=dvol.data_ptr())
+        else:
+            vt.generate_volume(vt.VT_GEN_BLOBS, cfg["seed"], (n, n, n), (256, 20.0, 120.0, 0.5, 1.5, 0.05),
+                               device_ptr=dvol.data_ptr())
+        torch.cuda.synchronize()
+        t1 = time.time()
+        self.octree_path = os.path.join(workdir, "vol_%s.oct" % cfg["gen"])
+        vt.build_octree_device(dvol.data_ptr(), vt.VT_F32, (n, n, n), cfg["iso"], self.octree_path)
+        t2 = time.time()
+        # host copy of the volume: the out-of-core source and the CPU baseline's input
+        self.host = torch.empty(n * n * n, dtype=torch.float32, pin_memory=True)
+        self.host.copy_(dvol)
+        torch.cuda.synchronize()
+        del dvol
+        torch.cuda.empty_cache()
+        self.volume = self.host.numpy().reshape(n, n, n)
+        t3 = time.time()
+        log("setup: generate %.1fs octree %.1fs host copy %.1fs" % (t1 - t0, t2 - t1, t3 - t2))
+        self.r = None
+        if need_renderer:
+            self.fm = vt.FileManager.wrap(self.volume)
+            self.oc = vt.Octree(self.octree_path)
+            edge = 1 << (self.oc.nLevels - cfg["levelC"])
+            D = edge + 2 * cfg["inc"]
+            slot = (D ** 3 * 4 + 15) // 16 * 16
+            dev = cfg.get("dev_bytes", 0) // slot or 8 ** cfg["levelC"]
+            host = cfg.get("host_bytes", 0) // slot or 8 ** cfg["levelC"]
+            self.slots = (dev, host, slot)
+            p = vt.make_params(W=cfg["W"], H=cfg["H"], octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"],
+                               levelCubes=cfg["levelC"], dimCube=edge, cubeInc=cfg["inc"], distance=cfg["dist"],
+                               fov_H=cfg["fov"], fov_W=cfg["fov"], maxElementsCache=dev, maxElementsCache_CPU=host)
+            opt = vt.default_options(resident=cfg["resident"], record_hits=0, host_threads=0)
+            t4 = time.time()
+            self.r = vt.visualTur(p, opt, volume=self.fm, octree=self.oc)
+            log("setup: renderer %.1fs (device slots %d, host slots %d, %d B/brick)" % (time.time() - t4, dev, host, slot))
+
+
+def roofline(stats_frames, trace_ms, pixels):
+    """Algorithmic bytes of the march (4 B voxels, 8 taps per sample, 6 extra
+    samples per hit for the normal) + 4 B per output pixel, over the trace
+    kernels' device time."""
+    samples = sum(s["samples"] for s in stats_frames)
+    hits = sum(s["hits"] for s in stats_frames)
+    b_alg = 4 * 8 * (samples + 6 * hits) + 4 * pixels
+    peak, src = HBM_FALLBACK_GBS, "fallback"
+    try:
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, src = float(mp["hbm_gbs"]), "measured"
+    except Exception:
+        pass
+    ach = b_alg / (trace_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": round(ach / peak, 4), "traffic": None, "bytes_alg_per_frame": b_alg / len(stats_frames),
+            "kernel": "k_trace"}
+
+
+def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, frame=0):
+    """Oracle (CPU restatement of the reference algorithm) on a bounded ray
+    sample of frame `frame`; returns rays/s."""
+    from oracle import oracle as orc
+    import visualtur_b200 as vt
+    o = orc.Octree(octree_path)
+    c = frame_camera(vt, cfg, frame)
+    cam = orc.Camera(cfg["H"], cfg["W"], cfg["dist"], cfg["fov"], cfg["fov"])
+    for f in ("look", "up", "right", "position"):
+        v = getattr(c, f)
+        setattr(cam.c, f, orc.orc_f3(v[0], v[1], v[2]))
+    n = cfg["W"] * cfg["H"]
+    stride = 1
+    # probe a sparse sample, then size the sample to the time budget
+    t0 = time.perf_counter()
+    orc.render(o, wl.volume, cam, cfg["levelO"], cfg["levelC"], cfg["inc"], nthreads=nthreads, ray_stride=257)
+    dt = max(time.perf_counter() - t0, 1e-6)
+    per_ray = dt / (n // 257 + 1)
+    stride = max(1, int(math.ceil(n * per_ray / budget_s)))
+    t0 = time.perf_counter()
+    reps = 0
+    rays = 0
+    while True:
+        orc.render(o, wl.volume, cam, cfg["levelO"], cfg["levelC"], cfg["inc"], nthreads=nthreads, ray_stride=stride)
+        rays += (n + stride - 1) // stride
+        reps += 1
+        if time.perf_counter() - t0 > budget_s * 0.5 or stride > 1:
+            break
+    el = time.perf_counter() - t0
+    threads = nthreads or os.cpu_count()
+    return {"value": round(rays / el, 1), "unit": "rays/s", "cores": threads, "kind": "port",
+            "sample": "%d x every %d-th ray of frame %d (%d rays, %.1f s)" % (reps, stride, frame, rays, el)}
+
+
+# ----------------------------------------------------------------------------- arms
+def run_ours(args, cfg, rank, world, torch, dist):
+    vt_dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(vt_dev)
+    work = tempfile.mkdtemp(prefix="vtbench_")
+    wl = Workload(cfg, torch, vt_dev, work)
+    r = wl.r
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    W, H = cfg["W"], cfg["H"]
+    rgba = torch.empty(W * H * 4, dtype=torch.float32, device=vt_dev)
+    rgb8 = torch.empty(W * H * 3, dtype=torch.uint8, device=vt_dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=vt_dev) if cfg["l2flush"] else None
+    frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
+    for i in range(args.warmup):
+        r.set_camera(frame_camera(wl.vt, cfg, frame0 + i))
+        r.updateVisibleCubes(rgba, rgb8, stream=sp)
+    torch.cuda.synchronize()
+    r.reset_stats()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(vt_dev.index)
+    per_frame = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for i in range(args.steps):
+        if flush is not None:
+            flush.zero_()
+        r.set_camera(frame_camera(wl.vt, cfg, frame0 + args.warmup + i))
+        ev[i][0].record(stream)
+        r.updateVisibleCubes(rgba, rgb8, stream=sp)
+        ev[i][1].record(stream)
+        per_frame.append(r.stats())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    tot_ms = sum(ms)
+    st = r.stats()
+    trace_ms = st["ms_trace_last_frame"]
+    # per-frame trace time: stats are cumulative except the last-frame fields
+    trace_tot = 0.0
+    prev = None
+    frames_stats = []
+    for s in per_frame:
+        trace_tot += s["ms_trace_last_frame"]
+        d = dict(s) if prev is None else {k: s[k] - prev[k] if isinstance(s[k], int) else s[k] for k in s}
+        frames_stats.append(d)
+        prev = s
+    rays_rank = W * H * args.steps
+    t_max = tot_ms
+    if dist:
+        t = torch.tensor([tot_ms], device=vt_dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = rays_rank * world / (t_max * 1e-3)
+    # end to end: public API with host output buffers (pose in, RGB8 image out)
+    e2e_steps = max(2, min(args.steps, 10))
+    out8 = np.empty((W * H, 3), np.uint8)
+    import ctypes
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        r.set_camera(frame_camera(wl.vt, cfg, frame0 + args.warmup + args.steps + i))
+        wl.vt.check(wl.vt.lib().vt_render_host(r._h, None, out8.ctypes.data))
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": round(W * H * e2e_steps / e2e_s * world, 1), "unit": "rays/s",
+           "h2d_bytes_per_step": ctypes.sizeof(wl.vt.vt_camera), "d2h_bytes_per_step": W * H * 3,
+           "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3)}
+    if rank != 0:
+        return None
+    line = {
+        "metric": "rays/s & ms/frame on 1 B200 (plain LRU renderer, single view)" if cfg["orbit"] else
+                  "rays/s & ms/frame on 1 B200 (resident march)",
+        "value": round(value, 1), "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, device-generated)",
+        "config": {"workload": cfg["workload"], "name": args.config, "W": W, "H": H,
+                   "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": roofline(frames_stats, trace_tot, W * H * args.steps),
+        "e2e": e2e,
+        "clocks": clk,
+        "gpu_launches": int(st["launches"]),
+        "frame_stats": {k: st[k] for k in ("passes", "bricks_requested", "bricks_loaded_disk", "host_hits",
+                                           "device_hits", "device_misses", "hits", "samples", "candidates")},
+        "ms_trace_total": round(trace_tot, 3),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, frame=frame0 + args.warmup)
+    return line
+
+
+def run_reference(args, cfg, rank, world, torch):
+    if rank != 0:
+        return None
+    dev = torch.device("cuda", 0)
+    work = tempfile.mkdtemp(prefix="vtbench_ref_")
+    wl = Workload(cfg, torch, dev, work, need_renderer=False)
+    n = cfg["W"] * cfg["H"]
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(cfg, wl, wl.octree_path, args.ref_budget, frame=i)
+        if i >= args.warmup:
+            vals.append(cb)
+    rays_s = statistics.median(v["value"] for v in vals)
+    line = {
+        "impl": "reference",
+        "metric": "rays/s & ms/frame on 1 B200 (plain LRU renderer, single view)" if cfg["orbit"] else
+                  "rays/s & ms/frame on 1 B200 (resident march)",
+        "value": rays_s, "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(n / rays_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": {"workload": cfg["workload"], "name": args.config, "W": cfg["W"], "H": cfg["H"]},
+        "cpu_baseline": dict(vals[-1], value=rays_s),
+        "e2e": {"value": rays_s, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's path is CUDA-only; this arm times its CPU restatement (oracle port) "
+                "on all host threads over a bounded ray sample per step",
+    }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default=os.environ.get("VT_BENCH_CONFIG", "c2"), choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--ref-budget", type=float, default=6.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        line = run_reference(args, cfg, rank, world, torch)
+    else:
+        line = run_ours(args, cfg, rank, world, torch, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

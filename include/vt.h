@@ -1,0 +1,226 @@
+/*
+ * vt.h -- C ABI of libvt.so, the B200 (sm_100a) isosurface ray caster with
+ * the capabilities of carlosduelo/visualTur.
+ *
+ * Conventions (all entry points):
+ *   - every call returns a vt_status; nothing calls exit(); vt_last_error()
+ *     gives a message for the calling thread's last failure;
+ *   - device buffers passed in are borrowed and owned by the caller;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default);
+ *     work is stream-ordered, calls return once it is enqueued unless the
+ *     entry point says it synchronises;
+ *   - a handle belongs to one host thread at a time; the caller serialises
+ *     calls from other threads;
+ *   - voxel layout: x slowest, z fastest (index z + y*dz + x*dy*dz), as the
+ *     reference's HDF5 datasets ([x][y][z], src/FileManager.cu:86-167).
+ *
+ * Reference citations are path:line in carlosduelo/visualTur.
+ */
+#ifndef VT_H
+#define VT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VT_API_VERSION 1
+
+typedef enum {
+    VT_OK = 0,
+    VT_ERR_INVALID = 1,      /* bad argument or inconsistent parameters */
+    VT_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    VT_ERR_IO = 3,           /* file could not be opened/read/written */
+    VT_ERR_FORMAT = 4,       /* bad octree magic / volume header */
+    VT_ERR_NOMEM = 5,        /* host or device allocation failed */
+    VT_ERR_TIMEOUT = 6,      /* a bounded device wait or frame loop gave up */
+    VT_ERR_STACK = 7,        /* a ray's traversal stack overflowed */
+    VT_ERR_UNSUPPORTED = 8,  /* valid request this build does not handle */
+    VT_ERR_STATE = 9         /* call not valid in the handle's state */
+} vt_status;
+
+const char* vt_status_string(vt_status s);
+const char* vt_last_error(void);
+int vt_api_version(void);
+
+/* Voxel types.  The reference stores float32 only (H5T_IEEE_F32LE,
+ * src/FileManager.cu:155); uint8 is an extension for 4096^3 volumes. */
+enum { VT_F32 = 0, VT_U8 = 1 };
+
+/* ------------------------------------------------------------------------ */
+/* Volume I/O (replaces class FileManager, inc/FileManager.hpp:12-35)       */
+/* ------------------------------------------------------------------------ */
+typedef struct vt_volume vt_volume;
+
+/* FileManager::FileManager (src/FileManager.cu:11-37).  Opens a project raw
+ * volume file ("VTVOL001" header) or an HDF5 file holding one contiguous
+ * 3-D dataset; `dataset` names the HDF5 dataset (ignored for raw files). */
+vt_status vt_volume_open(const char* path, const char* dataset, vt_volume** out);
+/* Wraps caller-owned host memory as a volume (no copy; must outlive it). */
+vt_status vt_volume_wrap(const void* data, int vtype, const int64_t dims[3], vt_volume** out);
+void      vt_volume_close(vt_volume* v);
+vt_status vt_volume_info(const vt_volume* v, int64_t dims[3], int* vtype);
+/* FileManager::readHDF5_Voxel_Array (src/FileManager.cu:86-167): reads
+ * voxels [s,e) into out (|e-s| per axis, float32); parts outside the volume
+ * are 0. */
+vt_status vt_volume_read(const vt_volume* v, const int s[3], const int e[3], float* out);
+/* FileManager::readHDF5 (src/FileManager.cu:71-84): whole dataset. */
+vt_status vt_volume_read_all(const vt_volume* v, void* out);
+/* FileManager::CreateFile (src/FileManager.cu:169-243).  format 0 = raw,
+ * 1 = HDF5 (contiguous dataset named `dataset`). */
+vt_status vt_volume_write(const char* path, const char* dataset, int format, const void* data,
+                          int vtype, const int64_t dims[3]);
+
+/* Seeded synthetic volumes (no reference counterpart).
+ *   VT_GEN_SPHERE: |x-c| + 0.25*g, g ~ N(0,1) by 4-term Irwin-Hall;
+ *                  params[0..2] = c; params[3] = noise sigma
+ *   VT_GEN_BLOBS:  sum of params[0] anisotropic Gaussian blobs, sigma in
+ *                  [params[1],params[2]], amplitude [params[3],params[4]],
+ *                  plus 4-octave value noise of amplitude params[5]
+ *   VT_GEN_FRACTAL_U8: 6-octave value noise in [0,255] with params[0]
+ *                  spheres of value params[3], radius [params[1],params[2]]
+ * Host generation writes `out` (host); device generation writes `dev_out`. */
+enum { VT_GEN_SPHERE = 0, VT_GEN_BLOBS = 1, VT_GEN_FRACTAL_U8 = 2 };
+vt_status vt_generate_volume(int kind, uint64_t seed, const int64_t dims[3], const float* params,
+                             int nparams, void* out);
+vt_status vt_generate_volume_device(int kind, uint64_t seed, const int64_t dims[3],
+                                    const float* params, int nparams, void* dev_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Octree (replaces class Octree, inc/Octree.hpp:12-42, and OctreeM,        */
+/* inc/CreateOctree.hpp:12-89)                                              */
+/* ------------------------------------------------------------------------ */
+typedef struct vt_octree vt_octree;
+
+/* Octree::Octree file reading (src/Octree.cu:769-813). */
+vt_status vt_octree_load(const char* path, vt_octree** out);
+void      vt_octree_free(vt_octree* o);
+vt_status vt_octree_info(const vt_octree* o, float* iso, int* dimension, int realDim[3], int* nLevels);
+/* Number of uint64 words of level `level` and a copy of them. */
+vt_status vt_octree_level(const vt_octree* o, int level, int64_t* n, uint64_t* words);
+/* OctreeM::OctreeM + writeToFile (src/CreateOctree.cu:300-371) on the GPU:
+ * builds the octree of `v` for isovalue `iso` and writes the file. */
+vt_status vt_octree_build(const vt_volume* v, float iso, const char* out_path, void* stream);
+/* Same for a volume already in device memory (dims[0]*dims[1]*dims[2]
+ * voxels of vtype, x slowest). */
+vt_status vt_octree_build_device(const void* dev_vol, int vtype, const int64_t dims[3], float iso,
+                                 const char* out_path, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Camera rays and single-brick rendering (class Camera, rayCaster)         */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int W, H;
+    float distance;          /* screen distance (Screen, src/Screen.cpp:11-20) */
+    float h, w;              /* screen extent in world units */
+    float look[3], up[3], right[3], position[3];
+} vt_camera;
+
+/* Camera(...) initial state (src/Camera.cu:12-29): fov_H/fov_W act as
+ * half-angles, h = 2*d*tanf(fov_H*pi/180). */
+vt_status vt_camera_init(vt_camera* c, int H, int W, float distance, float fov_H, float fov_W);
+/* Camera::Move/RotateX/RotateY/RotateZ/MoveForward/MoveUpward/StrafeRight
+ * (src/Camera.cu:85-156), including the reference's axis naming. op:
+ * 0 move(x,y,z) 1 rotX 2 rotY 3 rotZ 4 forward 5 upward 6 strafe. */
+vt_status vt_camera_op(vt_camera* c, int op, float a, float b, float cc);
+/* cuda_updateRays (src/Camera.cu:39-83): W*H float3 directions. */
+vt_status vt_camera_rays(const vt_camera* c, float* dev_dirs, void* stream);
+/* rayCaster::renderCube / cuda_rayCasterCube (src/rayCaster.cu:267-394):
+ * renders one brick of (cubeDim+2*cubeInc) voxels (float32, on device)
+ * whose interior starts at minBox, into dev_rgba (W*H*4 floats). */
+vt_status vt_render_cube(const vt_camera* c, const float* dev_cube, const int minBox[3],
+                         const int cubeDim[3], const int cubeInc[3], float iso, const float light[3],
+                         float* dev_rgba, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Renderer (replaces class visualTur, inc/visualTur.hpp:12-80)              */
+/* ------------------------------------------------------------------------ */
+/* visualTurParams_t (inc/visualTur.hpp:12-33). */
+typedef struct {
+    int W, H;
+    float distance, fov_H, fov_W;
+    int numRayPx;                 /* must be 1: the reference writes W*H rays only */
+    int maxElementsCache;         /* device brick slots */
+    int maxElementsCache_CPU;     /* pinned host brick slots */
+    int dimCubeCache[3];          /* brick edge; must equal 2^(nLevels-levelCubes) */
+    int cubeInc;                  /* apron; >= 3 so every tap stays in the brick */
+    int levelCubes;
+    const char* hdf5File;
+    const char* dataset_name;
+    const char* octreeFile;
+    int octreeLevel;
+} vt_params;
+
+/* Renderer options (no reference counterpart). */
+typedef struct {
+    int resident;          /* 1: whole volume in HBM, no brick cache; 0: brick cache */
+    int tile_w, tile_h;    /* pixels per CTA tile (autotuned) */
+    int unroll;            /* march unroll (autotuned) */
+    int lookahead;         /* bricks a suspended ray may request ahead (0..4) */
+    int max_passes;        /* bound on demand passes per frame */
+    int host_threads;      /* host tier fill threads (0 = hardware) */
+    int record_trace;      /* log per-frame touched coarse nodes */
+    int trace_level;       /* octree level of the logged nodes (4 in C4) */
+    int record_hits;       /* keep per-ray hit node/brick/t/normal for vt_debug_hits */
+} vt_options;
+
+typedef struct vt_handle vt_handle;
+
+void      vt_default_options(vt_options* o);
+/* visualTur::visualTur (src/visualTur.cu:10-35). */
+vt_status vt_create(const vt_params* p, const vt_options* opt, vt_handle** out);
+/* Same, with an already-open volume and loaded octree (borrowed). */
+vt_status vt_create_from(const vt_params* p, const vt_options* opt, vt_volume* v, vt_octree* o,
+                         vt_handle** out);
+void      vt_destroy(vt_handle* h);
+
+/* visualTur::camera_* (src/visualTur.cu:124-165); op codes as vt_camera_op. */
+vt_status vt_camera_update(vt_handle* h, int op, float a, float b, float c);
+/* Sets/reads the full camera state (extension: poses set directly). */
+vt_status vt_set_camera(vt_handle* h, const vt_camera* c);
+vt_status vt_get_camera(vt_handle* h, vt_camera* c);
+/* visualTur::changeScreen / changeNumRays / changeCacheParameters
+ * (src/visualTur.cu:83-122). */
+vt_status vt_change_screen(vt_handle* h, int W, int H, float fovW, float fovH, float distance);
+vt_status vt_change_num_rays(vt_handle* h, int numRayPx);
+vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], int cubeInc);
+
+/* visualTur::updateVisibleCubes (src/visualTur.cu:167-228): renders the
+ * current camera into dev_rgba (W*H*4 floats, pixel i*W+j) and, if not
+ * NULL, dev_rgb8 (W*H*3 bytes, (uint8)(clamp(v,0,1)*255)). */
+vt_status vt_render(vt_handle* h, float* dev_rgba, uint8_t* dev_rgb8, void* stream);
+/* Same with host output buffers (copies included); synchronises. */
+vt_status vt_render_host(vt_handle* h, float* host_rgba, uint8_t* host_rgb8);
+
+/* Many views in one persistent ray-queue launch (no reference counterpart). */
+typedef struct {
+    vt_camera cam;
+    float* dev_rgba;        /* W*H*4 floats, may be NULL if dev_rgb8 given */
+    uint8_t* dev_rgb8;      /* W*H*3 bytes, may be NULL */
+} vt_view;
+vt_status vt_render_batch(vt_handle* h, const vt_view* views, int n, void* stream);
+
+/* Per-ray diagnostics of the last vt_render (host buffers, W*H entries,
+ * any may be NULL): hit node Morton code at octreeLevel (0 = none), brick
+ * code at levelCubes, hit distance along the ray, unit normal. */
+vt_status vt_debug_hits(vt_handle* h, uint64_t* node_id, uint64_t* brick_id, float* t, float* normal);
+
+typedef struct {
+    int64_t frames, rays, hits, samples, normal_samples, candidates, expansions;
+    int64_t passes;                 /* demand passes in the last frame */
+    int64_t bricks_requested, bricks_loaded_host, bricks_loaded_disk, bricks_prefetched;
+    int64_t device_hits, device_misses, host_hits, host_misses;
+    int64_t max_stack;
+    int64_t launches;               /* libvt kernels launched (cumulative) */
+    double  ms_last_frame, ms_stall_last_frame, bytes_h2d_last_frame;
+    double  ms_trace_last_frame;    /* device time of the trace kernels of the last frame */
+} vt_stats;
+vt_status vt_get_stats(vt_handle* h, vt_stats* s);
+vt_status vt_reset_stats(vt_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,289 @@
+/*
+ * cache.cu -- two-tier brick cache (see cache.h).
+ *
+ * Semantics kept from lruCache (src/lruCache.cu:168-313): a brick is the
+ * zero-padded box [min - inc, min + edge + inc) of the volume, its id is
+ * the candidate id shifted to the brick level (:177), the device tier is
+ * filled from the host tier, the host tier from the volume, both evict the
+ * least recently used entry, and admission per pass is capped by the tier
+ * sizes (rays over the cap retry in the next pass, as NOCACHED rays do).
+ * Unlike the reference, a slot handed out in a pass is never evicted within
+ * that pass (the reference can, src/lruCache.cu:184,:256).
+ */
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+
+#include <omp.h>
+
+#include "cache.h"
+#include "vt_math.cuh"
+
+namespace vtrt {
+
+#define CKC(call)                                                                             \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(VT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+/* one CTA per brick: 16-byte copies from mapped host memory */
+__global__ void k_fill_bricks(const unsigned char* __restrict__ tier, size_t slotBytes, const int2* __restrict__ pairs,
+                              unsigned char* __restrict__ slab) {
+    int2 p = pairs[blockIdx.x];
+    const uint4* src = (const uint4*)(tier + (size_t)p.x * slotBytes);
+    uint4* dst = (uint4*)(slab + (size_t)p.y * slotBytes);
+    size_t n = slotBytes / 16;
+    for (size_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+/* page-table / stamp updates: x = page index, y = value; slot stamps for
+ * loaded bricks */
+__global__ void k_page_update(int* page, const int2* upd, int n, unsigned int* stamp, unsigned int stampValue) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int2 u = upd[i];
+    page[u.x] = u.y;
+    if (u.y >= 0) stamp[u.y] = stampValue;
+}
+
+BrickCache::~BrickCache() {
+    cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_);
+    if (h_tier_) cudaFreeHost(h_tier_);
+    if (h_pairs_) cudaFreeHost(h_pairs_);
+    if (h_upd_) cudaFreeHost(h_upd_);
+    if (h_req_) cudaFreeHost(h_req_);
+    cudaFree(d_pairs_); cudaFree(d_upd_);
+}
+
+vt_status BrickCache::init(const CacheConfig& c) {
+    cfg_ = c;
+    if (c.deviceSlots < 1) return fail(VT_ERR_INVALID, "maxElementsCache must be >= 1");
+    if (c.hostSlots < 1) return fail(VT_ERR_INVALID, "maxElementsCache_CPU must be >= 1");
+    esize_ = (int)c.vol->esize();
+    D_ = c.edge + 2 * c.inc;
+    slotBytes_ = ((size_t)D_ * D_ * D_ * esize_ + 15) & ~(size_t)15;
+    brickVol_ = slotBytes_ / esize_;
+    pageBase_ = 1ull << (3 * c.Lc);
+    pageN_ = (size_t)pageBase_;
+    nSlots_ = c.deviceSlots;
+    nHost_ = c.hostSlots;
+    CKC(cudaMalloc(&d_page_, pageN_ * 4));
+    CKC(cudaMemset(d_page_, 0xFF, pageN_ * 4));
+    CKC(cudaMalloc(&d_slab_, slotBytes_ * (size_t)nSlots_));
+    CKC(cudaMalloc(&d_stamp_, (size_t)nSlots_ * 4));
+    CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
+    CKC(cudaHostAlloc((void**)&h_tier_, slotBytes_ * (size_t)nHost_, cudaHostAllocMapped | cudaHostAllocPortable));
+    CKC(cudaHostGetDevicePointer(&d_tier_, h_tier_, 0));
+    slotBrick_.assign(nSlots_, 0);
+    stampHost_.assign(nSlots_, 0);
+    pageMirror_.assign(pageN_, -1);
+    hostIndex_.assign(pageN_, -1);
+    hostBrick_.assign(nHost_, 0);
+    hostTick_.assign(nHost_, 0);
+    return VT_OK;
+}
+
+void BrickCache::fill_args(DevBricks& b) const {
+    b.page = d_page_; b.pageBase = pageBase_; b.slab = d_slab_; b.D = D_; b.brickVol = (long long)brickVol_;
+    b.inc = cfg_.inc; b.vtype = cfg_.vol->vtype; b.stamp = d_stamp_; b.pass = pass_;
+}
+
+void BrickCache::read_brick(uint64_t code, void* dst) const {
+    int3 m = vt::min_box(code, cfg_.Lc, cfg_.nLevels);
+    int s[3] = {m.x - cfg_.inc, m.y - cfg_.inc, m.z - cfg_.inc};
+    int e[3] = {s[0] + D_, s[1] + D_, s[2] + D_};
+    volume_read_native(cfg_.vol, s, e, dst);
+}
+
+vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads) {
+    const size_t n = bricks.size();
+    hslot.assign(n, -1);
+    const uint64_t callStart = tick_ + 1;
+    std::vector<size_t> miss;
+    for (size_t i = 0; i < n; i++) {
+        int hs = hostIndex_[bricks[i] - pageBase_];
+        if (hs >= 0) { hslot[i] = hs; hostTick_[hs] = ++tick_; hostHits_++; }
+        else miss.push_back(i);
+    }
+    if (miss.empty()) return VT_OK;
+    /* victims: free host slots first, then least recently used, never a slot
+     * touched in this call */
+    std::vector<int> order(nHost_);
+    std::iota(order.begin(), order.end(), 0);
+    size_t want = miss.size();
+    if (want > (size_t)nHost_) return fail(VT_ERR_STATE, "host tier smaller than one request batch");
+    std::nth_element(order.begin(), order.begin() + (want - 1), order.end(), [&](int a, int b) {
+        bool fa = hostBrick_[a] == 0, fb = hostBrick_[b] == 0;
+        if (fa != fb) return fa;
+        return hostTick_[a] < hostTick_[b];
+    });
+    for (size_t k = 0; k < want; k++) {
+        int hs = order[k];
+        if (hostBrick_[hs] != 0 && hostTick_[hs] >= callStart) return fail(VT_ERR_STATE, "host tier exhausted");
+        if (hostBrick_[hs] != 0) hostIndex_[hostBrick_[hs] - pageBase_] = -1;
+        uint64_t b = bricks[miss[k]];
+        hostBrick_[hs] = b;
+        hostIndex_[b - pageBase_] = hs;
+        hostTick_[hs] = ++tick_;
+        hslot[miss[k]] = hs;
+    }
+    const int nth = cfg_.hostThreads;
+#pragma omp parallel for schedule(dynamic, 8) num_threads(nth > 0 ? nth : omp_get_max_threads())
+    for (long long k = 0; k < (long long)want; k++) {
+        size_t i = miss[k];
+        read_brick(bricks[i], h_tier_ + (size_t)hslot[i] * slotBytes_);
+    }
+    hostMisses_ += (int64_t)want;
+    *diskLoads += (int64_t)want;
+    return VT_OK;
+}
+
+vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
+                                    unsigned int protectFrom, double* h2d, int64_t* loaded) {
+    const size_t n = bricks.size();
+    if (n == 0) return VT_OK;
+    /* bricks with a host-tier copy, at most one per device slot */
+    size_t m = 0;
+    while (m < n && m < (size_t)nSlots_ && hslot[m] >= 0) m++;
+    size_t freeCount = 0;
+    for (int i = 0; i < nSlots_; i++) freeCount += slotBrick_[i] == 0;
+    if (freeCount < m) {
+        CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
+        CKC(cudaStreamSynchronize(s));
+    }
+    std::vector<int> order(nSlots_);
+    std::iota(order.begin(), order.end(), 0);
+    if (m > 0)
+        std::nth_element(order.begin(), order.begin() + (m - 1), order.end(), [&](int a, int b) {
+            bool fa = slotBrick_[a] == 0, fb = slotBrick_[b] == 0;
+            if (fa != fb) return fa;
+            return stampHost_[a] < stampHost_[b];
+        });
+    size_t need = n * 2 + 2;
+    if (need > updCap_) {
+        if (h_upd_) cudaFreeHost(h_upd_);
+        cudaFree(d_upd_);
+        updCap_ = need * 2;
+        CKC(cudaHostAlloc((void**)&h_upd_, updCap_ * sizeof(int2), cudaHostAllocDefault));
+        CKC(cudaMalloc(&d_upd_, updCap_ * sizeof(int2)));
+    }
+    if (n > pairsCap_) {
+        if (h_pairs_) cudaFreeHost(h_pairs_);
+        cudaFree(d_pairs_);
+        pairsCap_ = n * 2;
+        CKC(cudaHostAlloc((void**)&h_pairs_, pairsCap_ * sizeof(int2), cudaHostAllocDefault));
+        CKC(cudaMalloc(&d_pairs_, pairsCap_ * sizeof(int2)));
+    }
+    size_t nu = 0, np = 0;
+    for (size_t k = 0; k < m && np < m; k++) {
+        int slot = order[k];
+        if (slotBrick_[slot] != 0) {
+            if (stampHost_[slot] >= protectFrom) continue;   /* in use this frame */
+            uint64_t old = slotBrick_[slot];
+            pageMirror_[old - pageBase_] = -1;
+            h_upd_[nu++] = make_int2((int)(old - pageBase_), -1);
+        }
+        uint64_t b = bricks[np];
+        slotBrick_[slot] = b;
+        pageMirror_[b - pageBase_] = slot;
+        stampHost_[slot] = pass_ + 1;
+        h_upd_[nu++] = make_int2((int)(b - pageBase_), slot);
+        h_pairs_[np] = make_int2(hslot[np], slot);
+        np++;
+    }
+    /* requests that got no slot go back to absent (retried next pass) */
+    for (size_t k = np; k < n; k++)
+        if (pageMirror_[bricks[k] - pageBase_] < 0) h_upd_[nu++] = make_int2((int)(bricks[k] - pageBase_), -1);
+    if (np) {
+        launches_++;
+        CKC(cudaMemcpyAsync(d_pairs_, h_pairs_, np * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_fill_bricks<<<(unsigned int)np, 256, 0, s>>>((const unsigned char*)d_tier_, slotBytes_, d_pairs_,
+                                                       (unsigned char*)d_slab_);
+        CKC(cudaGetLastError());
+    }
+    if (nu) {
+        launches_++;
+        CKC(cudaMemcpyAsync(d_upd_, h_upd_, nu * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_page_update<<<(unsigned int)((nu + 255) / 256), 256, 0, s>>>(d_page_, d_upd_, (int)nu, d_stamp_, pass_ + 1);
+        CKC(cudaGetLastError());
+    }
+    /* the pinned lists are reused by the next call */
+    CKC(cudaStreamSynchronize(s));
+    *h2d += (double)np * (double)slotBytes_;
+    *loaded += (int64_t)np;
+    return VT_OK;
+}
+
+vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq, cudaStream_t s, double* h2dBytes) {
+    if (nReq == 0) return VT_OK;
+    if (nReq > reqCap_) {
+        if (h_req_) cudaFreeHost(h_req_);
+        reqCap_ = (size_t)nReq * 2;
+        CKC(cudaHostAlloc((void**)&h_req_, reqCap_ * 8, cudaHostAllocDefault));
+    }
+    CKC(cudaMemcpyAsync(h_req_, d_req, (size_t)nReq * 8, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    requested_ += nReq;
+    size_t cap = std::min<size_t>({(size_t)nReq, (size_t)nSlots_, (size_t)nHost_});
+    std::vector<uint64_t> bricks(h_req_, h_req_ + cap);
+    std::vector<int> hs;
+    int64_t disk = 0, loaded = 0;
+    vt_status st = ensure_host(bricks, hs, &disk);
+    if (st != VT_OK) return st;
+    /* bricks over the admission cap are re-requested next pass */
+    std::vector<uint64_t> all(h_req_, h_req_ + nReq);
+    std::vector<int> hsAll(hs);
+    hsAll.resize(nReq, -1);
+    /* assign_device handles the first `cap` and resets the rest */
+    st = assign_device(all, hsAll, s, 0xFFFFFFFFu, h2dBytes, &loaded);
+    return st;
+}
+
+vt_status BrickCache::prefetch(const std::vector<uint64_t>& bricks, cudaStream_t s, int64_t* loaded) {
+    std::vector<uint64_t> want;
+    for (uint64_t b : bricks)
+        if (pageMirror_[b - pageBase_] < 0) want.push_back(b);
+    size_t cap = std::min<size_t>({want.size(), (size_t)nSlots_, (size_t)nHost_});
+    want.resize(cap);
+    if (want.empty()) return VT_OK;
+    std::vector<int> hs;
+    int64_t disk = 0;
+    vt_status st = ensure_host(want, hs, &disk);
+    if (st != VT_OK) return st;
+    double h2d = 0;
+    int64_t got = 0;
+    /* never evict a slot used since the frame began */
+    st = assign_device(want, hs, s, frameStart_, &h2d, &got);
+    prefetched_ += got;
+    if (loaded) *loaded += got;
+    return st;
+}
+
+vt_status BrickCache::preload(const std::vector<uint64_t>& bricks) {
+    size_t batch = (size_t)std::min(nHost_, nSlots_);
+    int64_t loaded = 0;
+    double h2d = 0;
+    for (size_t i = 0; i < bricks.size(); i += batch) {
+        std::vector<uint64_t> b(bricks.begin() + i, bricks.begin() + std::min(bricks.size(), i + batch));
+        std::vector<int> hs;
+        int64_t disk = 0;
+        vt_status st = ensure_host(b, hs, &disk);
+        if (st != VT_OK) return st;
+        st = assign_device(b, hs, 0, 0xFFFFFFFFu, &h2d, &loaded);
+        if (st != VT_OK) return st;
+    }
+    allResident_ = (size_t)loaded == bricks.size() && bricks.size() <= (size_t)nSlots_;
+    return VT_OK;
+}
+
+void BrickCache::fold_stats(vt_stats& st) {
+    st.host_hits = hostHits_; st.host_misses = hostMisses_;
+    st.bricks_requested = requested_; st.bricks_loaded_disk = hostMisses_;
+    st.bricks_loaded_host = hostHits_; st.bricks_prefetched = prefetched_;
+    st.launches += launches_ - launchesFolded_;
+    launchesFolded_ = launches_;
+}
+void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = 0; }
+
+}  // namespace vtrt

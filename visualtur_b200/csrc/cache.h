@@ -1,0 +1,87 @@
+/*
+ * cache.h -- two-tier brick cache of libvt.so (replaces class lruCache,
+ * inc/lruCache.hpp:16-97, src/lruCache.cu).
+ *
+ * Device tier: a slab of `deviceSlots` bricks of (edge + 2*inc)^3 voxels and
+ * a direct-mapped page table indexed by brick Morton code (8^levelCubes
+ * entries: slot >= 0, -1 absent, -2 requested this pass).  Kernels look
+ * bricks up with one load and request absent ones with one atomicCAS; each
+ * use stamps the slot with the pass number, and eviction between passes
+ * takes the least recently used slots.
+ * Host tier: `hostSlots` bricks in pinned, device-mapped memory with the
+ * same LRU rule; misses read the brick zero-padded from the volume source
+ * (FileManager::readHDF5_Voxel_Array semantics) on host threads.  A fill
+ * kernel copies host-tier bricks into their device slots over PCIe/C2C.
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "vt_kernels.h"
+#include "vt_runtime.h"
+
+namespace vtrt {
+
+struct CacheConfig {
+    const vt_volume* vol = nullptr;
+    int nLevels = 0, Lc = 0, inc = 3, edge = 0;
+    int deviceSlots = 0, hostSlots = 0, hostThreads = 0;
+};
+
+class BrickCache {
+public:
+    ~BrickCache();
+    vt_status init(const CacheConfig& c);
+    /* loads `bricks` (sorted codes) into device slots before any frame */
+    vt_status preload(const std::vector<uint64_t>& bricks);
+    bool all_resident() const { return allResident_; }
+    void fill_args(DevBricks& b) const;
+    unsigned int next_pass() { return ++pass_; }
+    void begin_frame() { frameStart_ = pass_ + 1; }
+    /* services the nReq brick requests of the last pass (d_req, device) */
+    vt_status service(const unsigned long long* d_req, unsigned int nReq, cudaStream_t s, double* h2dBytes);
+    /* loads bricks ahead of demand (prefetch); never evicts slots stamped
+     * in the current frame */
+    vt_status prefetch(const std::vector<uint64_t>& bricks, cudaStream_t s, int64_t* loaded);
+    void fold_stats(vt_stats& st);
+    void reset_stats();
+    int device_slots() const { return nSlots_; }
+    size_t slot_bytes() const { return slotBytes_; }
+
+private:
+    vt_status ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads);
+    vt_status assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
+                            unsigned int protectFrom, double* h2d, int64_t* loaded);
+    void read_brick(uint64_t code, void* dst) const;
+
+    CacheConfig cfg_;
+    int D_ = 0, esize_ = 4;
+    size_t brickVol_ = 0, slotBytes_ = 0;
+    uint64_t pageBase_ = 0; size_t pageN_ = 0;
+    int* d_page_ = nullptr;
+    void* d_slab_ = nullptr;
+    unsigned int* d_stamp_ = nullptr;
+    int nSlots_ = 0;
+    std::vector<uint64_t> slotBrick_;        /* device slot -> brick (0 free) */
+    std::vector<int> pageMirror_;            /* host copy of page (>= 0 or -1) */
+    std::vector<unsigned int> stampHost_;
+    /* host tier */
+    unsigned char* h_tier_ = nullptr; void* d_tier_ = nullptr; int nHost_ = 0;
+    std::vector<int> hostIndex_;             /* brick -> host slot or -1 */
+    std::vector<uint64_t> hostBrick_;        /* host slot -> brick (0 free) */
+    std::vector<uint64_t> hostTick_;
+    uint64_t tick_ = 0;
+    /* transfer lists */
+    int2* h_pairs_ = nullptr; int2* d_pairs_ = nullptr; size_t pairsCap_ = 0;
+    int2* h_upd_ = nullptr; int2* d_upd_ = nullptr; size_t updCap_ = 0;
+    unsigned long long* h_req_ = nullptr; size_t reqCap_ = 0;
+    unsigned int pass_ = 0, frameStart_ = 1;
+    bool allResident_ = false;
+    /* stats */
+    int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0;
+    int64_t launches_ = 0, launchesFolded_ = 0;
+};
+
+}  // namespace vtrt

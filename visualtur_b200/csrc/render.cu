@@ -1,0 +1,481 @@
+/*
+ * render.cu -- ray-casting kernels of libvt.so (sm_100a).
+ *
+ * k_trace fuses the reference's three per-iteration phases -- octree
+ * traversal (cuda_getFirtsVoxel, src/Octree.cu:620-739), cache lookup
+ * (lruCache::updateCube, src/lruCache.cu:168-296) and march + shade
+ * (cuda_rayCaster, src/rayCaster.cu:139-265) -- into one kernel: each ray
+ * walks its DFS, marches every candidate node whose brick is resident, and
+ * either finishes or suspends with its stack saved when a brick is absent.
+ * The result equals the reference's iterate-until-PAINTED loop: candidates
+ * are marched in the same DFS order and the first hit is shaded.
+ *
+ * Octree: a flattened node array with 8-bit child masks holding the result
+ * of the reference's range search (computed once per octree load), so a
+ * traversal step is 8 slab tests and a popcount instead of binary searches.
+ */
+#include "vt_kernels.h"
+#include "vt_math.cuh"
+
+namespace vt {
+
+/* ---- samplers: voxel at brick-relative integer coordinates ------------- */
+template <int VTYPE>
+__device__ __forceinline__ float ldv(const void* p, long long i) {
+    if (VTYPE == 0) return __ldg((const float*)p + i);
+    return (float)__ldg((const unsigned char*)p + i);
+}
+
+/* Trilinear sampler over one brick (slab mode) or the padded volume
+ * (dense mode).  ox,oy,oz: integer origin of the index space (the
+ * reference's minBox = brick min corner - cubeInc); lo/hi: clamp range of
+ * the first tap so both taps stay inside the buffer (never active for
+ * finite positions with cubeInc >= 3). */
+struct Samp {
+    const void* base; long long sx, sy; int ox, oy, oz; int hx, hy, hz;
+};
+
+/* getElementInterpolate (src/rayCaster.cu:86-106). */
+template <int VTYPE>
+__device__ __forceinline__ float interp(const Samp& s, float3 p) {
+    float rx, ry, rz;
+    float px = modff(p.x, &rx), py = modff(p.y, &ry), pz = modff(p.z, &rz);
+    int x0 = f2i(rx - (float)s.ox), y0 = f2i(ry - (float)s.oy), z0 = f2i(rz - (float)s.oz);
+    x0 = min(max(x0, 0), s.hx); y0 = min(max(y0, 0), s.hy); z0 = min(max(z0, 0), s.hz);
+    long long b = (long long)x0 * s.sx + (long long)y0 * s.sy + z0;
+    float v000 = ldv<VTYPE>(s.base, b), v001 = ldv<VTYPE>(s.base, b + 1);
+    float v010 = ldv<VTYPE>(s.base, b + s.sy), v011 = ldv<VTYPE>(s.base, b + s.sy + 1);
+    float v100 = ldv<VTYPE>(s.base, b + s.sx), v101 = ldv<VTYPE>(s.base, b + s.sx + 1);
+    float v110 = ldv<VTYPE>(s.base, b + s.sx + s.sy), v111 = ldv<VTYPE>(s.base, b + s.sx + s.sy + 1);
+    float qx = 1.0f - px, qy = 1.0f - py, qz = 1.0f - pz;
+    float c00 = v000 * qx + v100 * px;
+    float c01 = v001 * qx + v101 * px;
+    float c10 = v010 * qx + v110 * px;
+    float c11 = v011 * qx + v111 * px;
+    float c0 = c00 * qy + c10 * py;
+    float c1 = c01 * qy + c11 * py;
+    return c0 * qz + c1 * pz;
+}
+
+/* getNormal (src/rayCaster.cu:131-137). */
+template <int VTYPE>
+__device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
+    float gx = (interp<VTYPE>(s, f3(p.x - 1.0f, p.y, p.z)) - interp<VTYPE>(s, f3(p.x + 1.0f, p.y, p.z))) / 2.0f;
+    float gy = (interp<VTYPE>(s, f3(p.x, p.y - 1.0f, p.z)) - interp<VTYPE>(s, f3(p.x, p.y + 1.0f, p.z))) / 2.0f;
+    float gz = (interp<VTYPE>(s, f3(p.x, p.y, p.z - 1.0f)) - interp<VTYPE>(s, f3(p.x, p.y, p.z + 1.0f))) / 2.0f;
+    return normalize(f3(gx, gy, gz));
+}
+
+/* The march of cuda_rayCaster (src/rayCaster.cu:166-237): samples at
+ * Xnear, Xnear += 0.5*dir, for steps 0..maxStep; the first sign change of
+ * iso - value (equality counts) is refined once linearly. */
+template <int VTYPE>
+__device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, float tnear,
+                                      int maxStep, float iso, float3* Xhit, unsigned int* nsamp) {
+    float3 Xnear = add(origin, mul(ray, tnear));
+    float3 Xfar = Xnear;
+    float3 vStep = mul(ray, 0.5f);
+    if (maxStep < 0) return false;
+    float ant = interp<VTYPE>(s, Xnear);
+    unsigned int ns = 1;
+    bool hit = false;
+    for (int steps = 1; steps <= maxStep; steps++) {
+        Xnear = add(Xnear, vStep);
+        float sig = interp<VTYPE>(s, Xnear);
+        ns++;
+        if ((((iso - ant) < 0.0f) && ((iso - sig) < 0.0f)) ||
+            (((iso - ant) > 0.0f) && ((iso - sig) > 0.0f))) {
+            ant = sig;
+            Xfar = Xnear;
+        } else {
+            float a = (iso - ant) / (sig - ant);
+            *Xhit = add(mul(Xfar, 1.0f - a), mul(Xnear, a));
+            hit = true;
+            break;
+        }
+    }
+    *nsamp += ns;
+    return hit;
+}
+
+/* Stack entry: (node index in its level << code_bits) | Morton code. */
+struct Stk {
+    unsigned long long e[VT_STACK];
+};
+
+template <int VTYPE, bool SLAB>
+__device__ __forceinline__ void setup_sampler(const TraceArgs& A, unsigned long long brick, Samp& s,
+                                              int* slot) {
+    const DevBricks& B = A.br;
+    if (SLAB) {
+        int3 bm = min_box(brick, A.oct.Lc, A.oct.nLevels);
+        s.ox = bm.x - B.inc; s.oy = bm.y - B.inc; s.oz = bm.z - B.inc;
+        int sl = B.page[brick - B.pageBase];
+        *slot = sl;
+        if (sl < 0) return;
+        s.base = (const char*)B.slab + (size_t)sl * (size_t)B.brickVol * (VTYPE == 0 ? 4 : 1);
+        s.sx = (long long)B.D * B.D; s.sy = B.D;
+        s.hx = s.hy = s.hz = B.D - 2;
+    } else {
+        /* dense: index space = the padded volume, global voxel g at g + P.
+         * Equals the brick-relative index of the reference whenever every
+         * tap lies inside the brick and its apron (cubeInc >= 3). */
+        *slot = 0;
+        s.ox = s.oy = s.oz = -B.P;
+        s.base = B.vol;
+        s.sx = B.vsx; s.sy = B.vsy;
+        s.hx = s.hy = s.hz = B.ve - 2;
+    }
+}
+
+struct RayOut {
+    float4 rgba; unsigned long long node, brick; float t; float3 n; bool hit;
+};
+
+/* Runs one ray's DFS from its stack until it finishes (returns true) or
+ * suspends on an absent brick (returns false; stack holds the state). */
+template <int VTYPE, bool SLAB>
+__device__ bool trace_ray(const TraceArgs& A, const RayInv& r, float3 dir, Stk& st, int& top,
+                          RayOut& o, unsigned int* cnt) {
+    const DevOctree& O = A.oct;
+    const int nLevels = O.nLevels, Lo = O.Lo;
+    const int codeBits = 3 * Lo + 1;
+    const unsigned long long codeMask = (1ull << codeBits) - 1ull;
+    const int dimO = 1 << (nLevels - Lo);
+    const int shiftOC = 3 * (Lo - O.Lc);
+    while (top >= 0) {
+        unsigned long long ent = st.e[top];
+        unsigned long long code = ent & codeMask;
+        unsigned int idx = (unsigned int)(ent >> codeBits);
+        int level = code_level(code);
+        int3 mb = min_box(code, level, nLevels);
+        if (level == Lo) {
+            /* candidate: brick lookup (lruCache::updateCube :177-291) */
+            unsigned long long brick = code >> shiftOC;
+            Samp s; int slot;
+            setup_sampler<VTYPE, SLAB>(A, brick, s, &slot);
+            if (SLAB && slot < 0) {
+                if (slot == -1) {
+                    int old = atomicCAS(&A.br.page[brick - A.br.pageBase], -1, -2);
+                    if (old == -1) {
+                        unsigned int q = atomicAdd(A.ctl.n_req, 1u);
+                        if (q < A.ctl.req_cap) A.ctl.req[q] = brick;
+                        else atomicOr(A.ctl.err, VT_KERR_REQUEST_FULL);
+                    }
+                }
+                cnt[VT_C_DEVMISSES]++;
+                return false;   /* suspend with the candidate still on top */
+            }
+            top--;
+            cnt[VT_C_CANDIDATES]++;
+            if (SLAB) { cnt[VT_C_DEVHITS]++; A.br.stamp[slot] = A.br.pass; }
+            float tn, tf;
+            if (!slab(r, mb.x, mb.y, mb.z, mb.x + dimO, mb.y + dimO, mb.z + dimO, &tn, &tf)) continue;
+            float3 X;
+            unsigned int ns = 0;
+            bool h = march<VTYPE>(s, r.o, dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
+            cnt[VT_C_SAMPLES] += ns;
+            if (h) {
+                /* shade (src/rayCaster.cu:238-250) */
+                float3 n = normal_at<VTYPE>(s, X);
+                cnt[VT_C_NSAMPLES] += 6;
+                float3 l = normalize(sub(X, A.light));
+                float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
+                float a = X.y / 256.0f;
+                o.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
+                o.hit = true; o.node = code; o.brick = brick; o.n = n;
+                o.t = dot(sub(X, r.o), dir);
+                return true;
+            }
+            continue;
+        }
+        /* expansion: _cuda_searchChildrenValidAndHit2 (src/Octree.cu:375-532)
+         * with membership from the flattened child mask */
+        top--;
+        cnt[VT_C_EXPANSIONS]++;
+        uint2 nd = O.nodes[level][idx];
+        const int cl = level + 1;
+        const int cd = 1 << (nLevels - cl);
+        unsigned long long cent[8];
+        float ctn[8], ctf[8];
+        int nv = 0;
+        unsigned int m = nd.y;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if ((m >> k) & 1u) {
+                int bx = mb.x + ((k >> 2) & 1) * cd, by = mb.y + ((k >> 1) & 1) * cd, bz = mb.z + (k & 1) * cd;
+                float a, b;
+                if (slab(r, bx, by, bz, bx + cd, by + cd, bz + cd, &a, &b) && b >= 0.0f) {
+                    unsigned long long cidx = nd.x + __popc(m & ((1u << k) - 1u));
+                    cent[nv] = (cidx << codeBits) | ((code << 3) + (unsigned long long)k);
+                    ctn[nv] = a; ctf[nv] = b;
+                    nv++;
+                }
+            }
+        }
+        /* bubble sort by (tnear, tfar), src/Octree.cu:665-706 */
+        int n = nv;
+        while (n != 0) {
+            int newn = 0;
+            for (int i = 1; i < nv; i++) {
+                if (ctn[i - 1] > ctn[i] || (ctn[i - 1] == ctn[i] && ctf[i - 1] > ctf[i])) {
+                    unsigned long long te = cent[i]; cent[i] = cent[i - 1]; cent[i - 1] = te;
+                    float tt = ctn[i]; ctn[i] = ctn[i - 1]; ctn[i - 1] = tt;
+                    tt = ctf[i]; ctf[i] = ctf[i - 1]; ctf[i - 1] = tt;
+                    newn = i;
+                }
+            }
+            n = newn;
+        }
+        if (top + nv >= VT_STACK) {
+            atomicOr(A.ctl.err, VT_KERR_STACK);
+            top = -1;
+            break;
+        }
+        for (int i = nv - 1; i >= 0; i--) st.e[++top] = cent[i];
+        if ((unsigned int)(top + 1) > cnt[VT_C_MAXSTACK]) cnt[VT_C_MAXSTACK] = top + 1;
+    }
+    return true;   /* exhausted: background */
+}
+
+template <int VTYPE, bool SLAB>
+__global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
+    unsigned int cnt[VT_C_COUNT];
+#pragma unroll
+    for (int c = 0; c < VT_C_COUNT; c++) cnt[c] = 0;
+    const DevCamera& C = A.cam;
+    int i = -1, j = -1, slotIn = -1;
+    if (A.ctl.susp_in == nullptr) {
+        int tw = A.tile_w, th = A.tile_h;
+        int tilesX = (C.W + tw - 1) / tw;
+        int tile = blockIdx.x * (blockDim.x / (tw * th)) + threadIdx.x / (tw * th);
+        int lt = threadIdx.x % (tw * th);
+        int ti = tile / tilesX, tj = tile % tilesX;
+        i = ti * th + lt / tw;
+        j = tj * tw + lt % tw;
+        if (i >= C.H || j >= C.W) i = -1;
+    } else {
+        unsigned int t = blockIdx.x * blockDim.x + threadIdx.x;
+        if (t < A.ctl.n_in) {
+            unsigned int id = A.ctl.susp_in[t];
+            i = id / C.W; j = id % C.W; slotIn = (int)t;
+        }
+    }
+    if (i >= 0) {
+        const int id = i * C.W + j;
+        float3 dir = ray_dir(C.look, C.up, C.right, C.dist, C.h, C.w, C.H, C.W, i, j);
+        RayInv r;
+        r.o = C.pos; r.dx = 1 / dir.x; r.dy = 1 / dir.y; r.dz = 1 / dir.z;
+        RayOut o;
+        o.rgba = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        o.hit = false; o.node = 0; o.brick = 0; o.t = -1.0f; o.n = f3(0, 0, 0);
+        Stk st;
+        int top = -1;
+        bool start = true;
+        if (slotIn >= 0) {
+            top = (int)A.ctl.top_in[slotIn] - 1;
+            for (int e = 0; e <= top; e++) st.e[e] = A.ctl.stk_in[(size_t)slotIn * VT_STACK + e];
+            start = false;
+        } else {
+            cnt[VT_C_RAYS]++;
+            const int N = 1 << A.oct.nLevels;
+            float tn, tf;
+            /* root test (src/Octree.cu:729) */
+            if (A.oct.rootValid && slab(r, 0, 0, 0, N, N, N, &tn, &tf)) { top = 0; st.e[0] = 1ull; }
+        }
+        (void)start;
+        bool done = trace_ray<VTYPE, SLAB>(A, r, dir, st, top, o, cnt);
+        if (done) {
+            if (o.hit) cnt[VT_C_HITS]++;
+            if (A.out.rgba) A.out.rgba[id] = o.rgba;
+            if (A.out.rgb8) {
+                A.out.rgb8[3 * (size_t)id] = to_u8(o.rgba.x);
+                A.out.rgb8[3 * (size_t)id + 1] = to_u8(o.rgba.y);
+                A.out.rgb8[3 * (size_t)id + 2] = to_u8(o.rgba.z);
+            }
+            if (A.out.node) A.out.node[id] = o.node;
+            if (A.out.brick) A.out.brick[id] = o.brick;
+            if (A.out.t) A.out.t[id] = o.t;
+            if (A.out.n) { A.out.n[3 * (size_t)id] = o.n.x; A.out.n[3 * (size_t)id + 1] = o.n.y; A.out.n[3 * (size_t)id + 2] = o.n.z; }
+        } else {
+            unsigned int q = atomicAdd(A.ctl.n_out, 1u);
+            if (q < A.ctl.susp_cap) {
+                A.ctl.susp_out[q] = (unsigned int)id;
+                A.ctl.top_out[q] = (unsigned char)(top + 1);
+                unsigned long long* dst = A.ctl.stk_out + (size_t)q * VT_STACK;
+                for (int e = 0; e <= top; e++) dst[e] = st.e[e];
+            } else {
+                atomicOr(A.ctl.err, VT_KERR_SUSPEND_FULL);
+            }
+            cnt[VT_C_SUSPENDED]++;
+        }
+    }
+    /* warp-aggregated counters */
+#pragma unroll
+    for (int c = 0; c < VT_C_COUNT; c++) {
+        unsigned int v = cnt[c];
+        if (c == VT_C_MAXSTACK) {
+            for (int off = 16; off; off >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, off));
+            if ((threadIdx.x & 31) == 0 && v) atomicMax(&A.ctl.counters[c], (unsigned long long)v);
+        } else {
+            for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if ((threadIdx.x & 31) == 0 && v) atomicAdd(&A.ctl.counters[c], (unsigned long long)v);
+        }
+    }
+}
+
+/* cuda_updateRays (src/Camera.cu:39-74) */
+__global__ void k_rays(DevCamera C, float* dirs) {
+    long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long long)C.W * C.H) return;
+    int i = (int)(id / C.W), j = (int)(id % C.W);
+    float3 d = ray_dir(C.look, C.up, C.right, C.dist, C.h, C.w, C.H, C.W, i, j);
+    dirs[3 * id] = d.x; dirs[3 * id + 1] = d.y; dirs[3 * id + 2] = d.z;
+}
+
+/* cuda_rayCasterCube (src/rayCaster.cu:267-357) */
+__device__ __forceinline__ float cube_get(const float* c, int D, long long total, int x, int y, int z) {
+    long long i = (long long)z + (long long)y * D + (long long)x * D * D;
+    if (i < 0 || i >= total) return 0.0f;   /* outside the allocation */
+    return __ldg(c + i);
+}
+__device__ __forceinline__ float cube_interp(const float* c, int D, long long total, int3 mb, float3 p) {
+    float rx, ry, rz;
+    float px = modff(p.x, &rx), py = modff(p.y, &ry), pz = modff(p.z, &rz);
+    int x0 = f2i(rx - (float)mb.x), y0 = f2i(ry - (float)mb.y), z0 = f2i(rz - (float)mb.z);
+    int x1 = x0 + 1, y1 = y0 + 1, z1 = z0 + 1;
+    float c00 = cube_get(c, D, total, x0, y0, z0) * (1.0f - px) + cube_get(c, D, total, x1, y0, z0) * px;
+    float c01 = cube_get(c, D, total, x0, y0, z1) * (1.0f - px) + cube_get(c, D, total, x1, y0, z1) * px;
+    float c10 = cube_get(c, D, total, x0, y1, z0) * (1.0f - px) + cube_get(c, D, total, x1, y1, z0) * px;
+    float c11 = cube_get(c, D, total, x0, y1, z1) * (1.0f - px) + cube_get(c, D, total, x1, y1, z1) * px;
+    float c0 = c00 * (1.0f - py) + c10 * py;
+    float c1 = c01 * (1.0f - py) + c11 * py;
+    return c0 * (1.0f - pz) + c1 * pz;
+}
+__global__ void k_cube(DevCamera C, const float* cube, int3 pmin, int3 cdim, int3 cinc, float iso,
+                       float3 light, float4* rgba) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long long)C.W * C.H) return;
+    int i = (int)(tid / C.W), j = (int)(tid % C.W);
+    float3 ray = ray_dir(C.look, C.up, C.right, C.dist, C.h, C.w, C.H, C.W, i, j);
+    RayInv r; r.o = C.pos; r.dx = 1 / ray.x; r.dy = 1 / ray.y; r.dz = 1 / ray.z;
+    int3 mb = pmin;
+    const int D = cdim.x + 2 * cinc.x;
+    const long long total = (long long)(cdim.x + 2 * cinc.x) * (cdim.y + 2 * cinc.y) * (cdim.z + 2 * cinc.z);
+    float tn, tf;
+    bool hit = false;
+    float3 Xnew = f3(0, 0, 0);
+    if (slab(r, mb.x, mb.y, mb.z, mb.x + cdim.x, mb.y + cdim.y, mb.z + cdim.z, &tn, &tf)) {
+        mb.x -= cinc.x; mb.y -= cinc.y; mb.z -= cinc.z;
+        float3 Xnear = add(C.pos, mul(ray, tn));
+        float3 Xfar = Xnear;
+        Xnew = Xnear;
+        bool primera = true;
+        float ant = 0.0f, sig = 0.0f;
+        float steps = 0;
+        float3 vStep = mul(ray, 0.5f);
+        float maxStep = (tf - tn) * 2.0f;   /* (tfar-tnear)/0.5, an exact doubling */
+        while (steps <= maxStep) {
+            if (primera) {
+                primera = false;
+                ant = cube_interp(cube, D, total, mb, Xnear);
+                Xfar = Xnear;
+            } else {
+                sig = cube_interp(cube, D, total, mb, Xnear);
+                if ((((iso - ant) < 0.0f) && ((iso - sig) < 0.0f)) ||
+                    (((iso - ant) > 0.0f) && ((iso - sig) > 0.0f))) {
+                    ant = sig;
+                    Xfar = Xnear;
+                } else {
+                    float a = (iso - ant) / (sig - ant);
+                    Xnew = add(mul(Xfar, 1.0f - a), mul(Xnear, a));
+                    hit = true;
+                    steps = maxStep;
+                }
+            }
+            Xnear = add(Xnear, vStep);
+            steps++;
+        }
+    }
+    float4 out = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+    if (hit) {
+        float gx = (cube_interp(cube, D, total, mb, f3(Xnew.x - 1.0f, Xnew.y, Xnew.z)) -
+                    cube_interp(cube, D, total, mb, f3(Xnew.x + 1.0f, Xnew.y, Xnew.z))) / 2.0f;
+        float gy = (cube_interp(cube, D, total, mb, f3(Xnew.x, Xnew.y - 1.0f, Xnew.z)) -
+                    cube_interp(cube, D, total, mb, f3(Xnew.x, Xnew.y + 1.0f, Xnew.z))) / 2.0f;
+        float gz = (cube_interp(cube, D, total, mb, f3(Xnew.x, Xnew.y, Xnew.z - 1.0f)) -
+                    cube_interp(cube, D, total, mb, f3(Xnew.x, Xnew.y, Xnew.z + 1.0f))) / 2.0f;
+        float3 n = normalize(f3(gx, gy, gz));
+        float3 l = normalize(sub(Xnew, light));
+        float dif = fabsf(dot(n, l));
+        float a = Xnew.y / (float)cdim.y;
+        out = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
+    }
+    rgba[tid] = out;
+}
+
+/* Copies a host-visible (mapped) volume into the zero-padded device copy. */
+template <int VTYPE>
+__global__ void k_fill_dense(void* dst, const void* src, long long nx, long long ny, long long nz, int P,
+                             long long ey, long long ez) {
+    long long row = blockIdx.x;   /* one (x,y) row per block */
+    long long x = row / ny, y = row % ny;
+    long long dbase = ((x + P) * ey + (y + P)) * ez + P;
+    long long sbase = (x * ny + y) * nz;
+    for (long long z = threadIdx.x; z < nz; z += blockDim.x) {
+        if (VTYPE == 0) ((float*)dst)[dbase + z] = ((const float*)src)[sbase + z];
+        else ((unsigned char*)dst)[dbase + z] = ((const unsigned char*)src)[sbase + z];
+    }
+}
+
+}  // namespace vt
+
+using namespace vt;
+
+cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, cudaStream_t s) {
+    const int threads = 128;
+    unsigned int blocks;
+    if (a.ctl.susp_in == nullptr) {
+        int per = threads / (a.tile_w * a.tile_h);
+        if (per < 1 || threads % (a.tile_w * a.tile_h)) return cudaErrorInvalidValue;
+        long long tiles = (long long)((a.cam.W + a.tile_w - 1) / a.tile_w) * ((a.cam.H + a.tile_h - 1) / a.tile_h);
+        blocks = (unsigned int)((tiles + per - 1) / per);
+    } else {
+        if (a.ctl.n_in == 0) return cudaSuccess;
+        blocks = (a.ctl.n_in + threads - 1) / threads;
+    }
+    if (blocks == 0) return cudaSuccess;
+    if (a.br.vtype == 0) {
+        if (slabMode) k_trace<0, true><<<blocks, threads, 0, s>>>(a);
+        else k_trace<0, false><<<blocks, threads, 0, s>>>(a);
+    } else {
+        if (slabMode) k_trace<1, true><<<blocks, threads, 0, s>>>(a);
+        else k_trace<1, false><<<blocks, threads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t vt_launch_rays(const DevCamera& c, float* dirs, cudaStream_t s) {
+    long long n = (long long)c.W * c.H;
+    if (n == 0) return cudaSuccess;
+    k_rays<<<(unsigned int)((n + 255) / 256), 256, 0, s>>>(c, dirs);
+    return cudaGetLastError();
+}
+
+cudaError_t vt_launch_cube(const DevCamera& c, const float* cube, int3 minBox, int3 cubeDim,
+                           int3 cubeInc, float iso, float3 light, float4* rgba, cudaStream_t s) {
+    long long n = (long long)c.W * c.H;
+    if (n == 0) return cudaSuccess;
+    k_cube<<<(unsigned int)((n + 127) / 128), 128, 0, s>>>(c, cube, minBox, cubeDim, cubeInc, iso, light, rgba);
+    return cudaGetLastError();
+}
+
+cudaError_t vt_launch_fill_dense(void* dst, int vtype, const void* src, long long nx, long long ny,
+                                 long long nz, int P, long long ey, long long ez, cudaStream_t s) {
+    long long rows = nx * ny;
+    if (rows == 0) return cudaSuccess;
+    if (rows > 2147483647LL) return cudaErrorInvalidValue;
+    if (vtype == 0) k_fill_dense<0><<<(unsigned int)rows, 256, 0, s>>>(dst, src, nx, ny, nz, P, ey, ez);
+    else k_fill_dense<1><<<(unsigned int)rows, 256, 0, s>>>(dst, src, nx, ny, nz, P, ey, ez);
+    return cudaGetLastError();
+}

@@ -1,0 +1,197 @@
+/*
+ * volume.cpp -- volume sources of libvt.so: the FileManager surface
+ * (inc/FileManager.hpp:12-35) over memory-mapped raw or HDF5 files, and the
+ * seeded synthetic volume generators.
+ */
+#include <fcntl.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cmath>
+#include <string>
+
+#include "vt_runtime.h"
+
+namespace vtrt {
+
+static thread_local std::string g_err;
+
+vt_status fail(vt_status s, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+void clear_error() { g_err.clear(); }
+const char* last_error() { return g_err.c_str(); }
+
+/* FileManager::readHDF5_Voxel_Array (src/FileManager.cu:86-167): output of
+ * |e-s| voxels per axis, zeroed; nothing is copied when the box lies
+ * completely outside; otherwise the overlap is copied at its offset. */
+template <class OutT>
+static void read_box(const vt_volume* v, const int s[3], const int e[3], OutT* out) {
+    int64_t dim[3];
+    for (int a = 0; a < 3; a++) dim[a] = std::llabs((long long)e[a] - s[a]);
+    memset(out, 0, (size_t)(dim[0] * dim[1] * dim[2]) * sizeof(OutT));
+    const int64_t* D = v->dims;
+    if (s[0] >= D[0] || s[1] >= D[1] || s[2] >= D[2] || e[0] < 0 || e[1] < 0 || e[2] < 0) return;
+    int64_t oo[3], off[3], dr[3];
+    for (int a = 0; a < 3; a++) {
+        oo[a] = s[a] < 0 ? -(int64_t)s[a] : 0;
+        off[a] = s[a] < 0 ? 0 : s[a];
+        dr[a] = e[a] > D[a] ? D[a] - off[a] : e[a] - off[a];
+        if (dr[a] <= 0) return;
+    }
+    for (int64_t a = 0; a < dr[0]; a++)
+        for (int64_t b = 0; b < dr[1]; b++) {
+            size_t src = (size_t)(((off[0] + a) * D[1] + (off[1] + b)) * D[2] + off[2]);
+            OutT* dst = out + ((oo[0] + a) * dim[1] + (oo[1] + b)) * dim[2] + oo[2];
+            if (v->vtype == VT_F32) {
+                const float* sp = (const float*)v->data + src;
+                if (sizeof(OutT) == 4) memcpy(dst, sp, (size_t)dr[2] * 4);
+                else for (int64_t c = 0; c < dr[2]; c++) dst[c] = (OutT)sp[c];
+            } else {
+                const uint8_t* sp = v->data + src;
+                if (sizeof(OutT) == 1) memcpy(dst, sp, (size_t)dr[2]);
+                else for (int64_t c = 0; c < dr[2]; c++) dst[c] = (OutT)sp[c];
+            }
+        }
+}
+
+void volume_read(const vt_volume* v, const int s[3], const int e[3], float* out) { read_box(v, s, e, out); }
+void volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out) {
+    if (v->vtype == VT_F32) read_box(v, s, e, (float*)out);
+    else read_box(v, s, e, (uint8_t*)out);
+}
+
+}  // namespace vtrt
+
+using namespace vtrt;
+
+/* ---- raw volume file: 64-byte header then voxels ----------------------- */
+/* "VTVOL001", u32 version 1, u32 voxel type, i64 dims[3], u64 data offset */
+static bool parse_raw(const unsigned char* p, size_t len, int* vtype, int64_t dims[3], uint64_t* off) {
+    if (len < 64 || memcmp(p, "VTVOL001", 8) != 0) return false;
+    uint32_t ver, vt;
+    memcpy(&ver, p + 8, 4); memcpy(&vt, p + 12, 4);
+    memcpy(dims, p + 16, 24); memcpy(off, p + 40, 8);
+    if (ver != 1 || (vt != VT_F32 && vt != VT_U8)) return false;
+    *vtype = (int)vt;
+    return true;
+}
+
+extern "C" vt_status vt_volume_open(const char* path, const char* dataset, vt_volume** out) {
+    clear_error();
+    if (!path || !out) return fail(VT_ERR_INVALID, "vt_volume_open: null argument");
+    int fd = open(path, O_RDONLY);
+    if (fd < 0) return fail(VT_ERR_IO, "unable to open the requested file %s", path);
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size < 64) { close(fd); return fail(VT_ERR_FORMAT, "file too small: %s", path); }
+    size_t len = (size_t)st.st_size;
+    void* base = mmap(nullptr, len, PROT_READ, MAP_SHARED, fd, 0);
+    close(fd);
+    if (base == MAP_FAILED) return fail(VT_ERR_IO, "mmap failed: %s", path);
+    const unsigned char* p = (const unsigned char*)base;
+    int vtype; int64_t dims[3]; uint64_t off;
+    std::string why;
+    bool ok = parse_raw(p, len, &vtype, dims, &off);
+    if (!ok) ok = h5_locate(p, len, dataset ? dataset : "value", &vtype, dims, &off, &why);
+    if (!ok) {
+        munmap(base, len);
+        return fail(VT_ERR_FORMAT, "unable to open the requested data set in %s: %s", path,
+                    why.empty() ? "not a raw volume or HDF5 file" : why.c_str());
+    }
+    size_t need = (size_t)dims[0] * dims[1] * dims[2] * (vtype == VT_U8 ? 1 : 4);
+    if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0 || off + need > len) {
+        munmap(base, len);
+        return fail(VT_ERR_FORMAT, "truncated volume %s", path);
+    }
+    vt_volume* v = new vt_volume();
+    v->vtype = vtype;
+    for (int a = 0; a < 3; a++) v->dims[a] = dims[a];
+    v->map_base = base; v->map_len = len; v->data = p + off; v->path = path;
+    madvise(base, len, MADV_WILLNEED);
+    *out = v;
+    return VT_OK;
+}
+
+extern "C" vt_status vt_volume_wrap(const void* data, int vtype, const int64_t dims[3], vt_volume** out) {
+    clear_error();
+    if (!data || !dims || !out) return fail(VT_ERR_INVALID, "vt_volume_wrap: null argument");
+    if (vtype != VT_F32 && vtype != VT_U8) return fail(VT_ERR_INVALID, "bad voxel type %d", vtype);
+    if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0) return fail(VT_ERR_INVALID, "bad dims");
+    vt_volume* v = new vt_volume();
+    v->vtype = vtype;
+    for (int a = 0; a < 3; a++) v->dims[a] = dims[a];
+    v->data = (const unsigned char*)data;
+    *out = v;
+    return VT_OK;
+}
+
+extern "C" void vt_volume_close(vt_volume* v) {
+    if (!v) return;
+    if (v->map_base) munmap(v->map_base, v->map_len);
+    delete v;
+}
+
+extern "C" vt_status vt_volume_info(const vt_volume* v, int64_t dims[3], int* vtype) {
+    clear_error();
+    if (!v) return fail(VT_ERR_INVALID, "null volume");
+    if (dims) for (int a = 0; a < 3; a++) dims[a] = v->dims[a];
+    if (vtype) *vtype = v->vtype;
+    return VT_OK;
+}
+
+extern "C" vt_status vt_volume_read(const vt_volume* v, const int s[3], const int e[3], float* out) {
+    clear_error();
+    if (!v || !s || !e || !out) return fail(VT_ERR_INVALID, "vt_volume_read: null argument");
+    volume_read(v, s, e, out);
+    return VT_OK;
+}
+
+extern "C" vt_status vt_volume_read_all(const vt_volume* v, void* out) {
+    clear_error();
+    if (!v || !out) return fail(VT_ERR_INVALID, "vt_volume_read_all: null argument");
+    memcpy(out, v->data, v->voxels() * v->esize());
+    return VT_OK;
+}
+
+extern "C" vt_status vt_volume_write(const char* path, const char* dataset, int format, const void* data,
+                                     int vtype, const int64_t dims[3]) {
+    clear_error();
+    if (!path || !data || !dims) return fail(VT_ERR_INVALID, "vt_volume_write: null argument");
+    if (vtype != VT_F32 && vtype != VT_U8) return fail(VT_ERR_INVALID, "bad voxel type %d", vtype);
+    size_t n = (size_t)dims[0] * dims[1] * dims[2] * (vtype == VT_U8 ? 1 : 4);
+    if (format == 1) {
+        std::string why;
+        if (!h5_write(path, dataset ? dataset : "value", data, vtype, dims, &why))
+            return fail(VT_ERR_IO, "unable to create the HDF5 file %s: %s", path, why.c_str());
+        return VT_OK;
+    }
+    FILE* f = fopen(path, "wb");
+    if (!f) return fail(VT_ERR_IO, "unable to create %s", path);
+    unsigned char h[64];
+    memset(h, 0, 64);
+    memcpy(h, "VTVOL001", 8);
+    uint32_t ver = 1, vt = (uint32_t)vtype;
+    uint64_t off = 64;
+    memcpy(h + 8, &ver, 4); memcpy(h + 12, &vt, 4); memcpy(h + 16, dims, 24); memcpy(h + 40, &off, 8);
+    bool ok = fwrite(h, 1, 64, f) == 64;
+    const unsigned char* p = (const unsigned char*)data;
+    size_t done = 0;
+    while (ok && done < n) {
+        size_t chunk = n - done < (size_t)(1u << 30) ? n - done : (size_t)(1u << 30);
+        ok = fwrite(p + done, 1, chunk, f) == chunk;
+        done += chunk;
+    }
+    if (fclose(f) != 0) ok = false;
+    return ok ? VT_OK : fail(VT_ERR_IO, "short write to %s", path);
+}

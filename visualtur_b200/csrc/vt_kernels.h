@@ -1,0 +1,89 @@
+/*
+ * vt_kernels.h -- argument blocks shared by the host runtime and the CUDA
+ * kernels of libvt.so (internal header; the public ABI is include/vt.h).
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define VT_MAX_LEVELS 20
+#define VT_STACK 64          /* per-ray DFS stack entries (reference: 32) */
+
+/* error bits reported by kernels through DevCtl::err */
+#define VT_KERR_STACK 1u        /* a ray's stack overflowed */
+#define VT_KERR_NOTRESIDENT 2u  /* resident mode met a brick with no slot */
+#define VT_KERR_SUSPEND_FULL 4u /* suspended-ray list overflowed */
+#define VT_KERR_REQUEST_FULL 8u /* brick request list overflowed */
+
+/* counter slots in DevCtl::counters */
+enum {
+    VT_C_RAYS = 0, VT_C_HITS, VT_C_SAMPLES, VT_C_NSAMPLES, VT_C_CANDIDATES, VT_C_EXPANSIONS,
+    VT_C_MAXSTACK, VT_C_SUSPENDED, VT_C_REQUESTS, VT_C_DEVHITS, VT_C_DEVMISSES, VT_C_COUNT
+};
+
+struct DevCamera {
+    float3 look, up, right, pos;
+    float h, w, dist;
+    int W, H;
+};
+
+/* Flattened octree: node records of levels 0..Lo-1.  node.x = index of the
+ * first child in the next level's array, node.y = 8-bit child mask (bit k =
+ * child (code<<3)+k accepted by the reference's range search). */
+struct DevOctree {
+    int nLevels, Lo, Lc, rootValid;
+    const uint2* nodes[VT_MAX_LEVELS];
+};
+
+/* Brick storage.  Dense: the whole zero-padded volume, P voxels of zeros on
+ * every side; index ((x+P)*ey + (y+P))*ez + (z+P).  Slab: bricks of D^3
+ * voxels (edge + 2*inc) in slots; page[code - pageBase] = slot or < 0. */
+struct DevBricks {
+    const void* vol;  long long vsx, vsy; int P; int ve;   /* ve: padded edge */
+    int* page; unsigned long long pageBase; const void* slab; int D; long long brickVol;
+    int inc; int vtype;
+    unsigned int* stamp;   /* per slot: last pass that used it (slab mode) */
+    unsigned int pass;
+};
+
+struct DevOut {
+    float4* rgba;
+    uint8_t* rgb8;
+    unsigned long long* node;
+    unsigned long long* brick;
+    float* t;
+    float* n;
+};
+
+/* Per-frame control: counters, error bits, demand paging queues. */
+struct DevCtl {
+    unsigned long long* counters;
+    unsigned int* err;
+    /* suspended rays: ray ids and saved stacks (in: this pass, out: next) */
+    const unsigned int* susp_in; unsigned int n_in;   /* rays to resume (NULL: all) */
+    const unsigned long long* stk_in; const unsigned char* top_in;
+    unsigned int* susp_out; unsigned int* n_out; unsigned int susp_cap;
+    unsigned long long* stk_out; unsigned char* top_out;
+    /* brick requests */
+    unsigned long long* req; unsigned int* n_req; unsigned int req_cap;
+    int lookahead;
+};
+
+struct TraceArgs {
+    DevCamera cam;
+    DevOctree oct;
+    DevBricks br;
+    DevOut out;
+    DevCtl ctl;
+    float iso;
+    float3 light;
+    int tile_w, tile_h;
+};
+
+/* launchers (render.cu) */
+cudaError_t vt_launch_trace(const TraceArgs& a, bool slab, cudaStream_t s);
+cudaError_t vt_launch_rays(const DevCamera& c, float* dirs, cudaStream_t s);
+cudaError_t vt_launch_cube(const DevCamera& c, const float* cube, int3 minBox, int3 cubeDim,
+                           int3 cubeInc, float iso, float3 light, float4* rgba, cudaStream_t s);
+cudaError_t vt_launch_fill_dense(void* dst, int vtype, const void* src, long long nx, long long ny,
+                                 long long nz, int P, long long ey, long long ez, cudaStream_t s);
