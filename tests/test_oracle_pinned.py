@@ -56,10 +56,12 @@ def test_render_matches_reference(case, workdir):
     ref_node = np.where(ref_hit, g["ids"], 0)
     ref_brick = np.where(ref_hit, g["cube"], 0)
     agree = ref_node == r["node"]
-    assert agree.mean() >= 0.995, "node agreement %.4f" % agree.mean()
+    # measured: every ray agrees; colours differ by <= 2 ulp (contraction and
+    # the hardware rsqrtf in the reference's device code)
+    assert agree.all(), "node agreement %.4f" % agree.mean()
     assert (ref_brick[agree] == r["brick"][agree]).all()
     both = agree & ref_hit
-    assert np.abs(g["rgba"][both] - r["rgba"][both]).max() < 2e-3
+    assert np.abs(g["rgba"][both] - r["rgba"][both]).max() < 1e-6
     ref8 = (np.clip(g["rgba"][:, :3], 0, 1) * 255).astype(np.uint8)
     assert np.abs(ref8[both].astype(int) - r["rgb8"][both].astype(int)).max() <= 1
     assert np.array_equal(g["rgba"][~ref_hit], r["rgba"][~ref_hit])   # background (1,1,1,1)
