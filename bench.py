@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark: rays/s and ms/frame of the isosurface ray caster on B200.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1|c2s] [--mode best|plain]
+                  [--impl ours|reference]
 
 A step is one rendered frame of the workload:
   c2 (default): the 2048^3 float32 out-of-core fly-through -- 256 seeded
@@ -43,10 +44,23 @@ CONFIGS = {
                gen="sphere", seed=1234, n=128, iso=40.0, levelC=4, levelO=5, inc=3, W=512, H=512, fov=30.0,
                dist=50.0, resident=1, l2flush=True, orbit=None, cam_pos=(63.5, 63.5, 363.5)),
     "c2": dict(workload="2048^3 f32 blobs+noise, iso 0.6, out-of-core: 16^3 bricks (apron 3), 4 GB device "
-                        "cache, 16 GB pinned host tier, 1920x1080, orbit r=3000 at 1.2 deg/frame",
+                        "cache, 16 GB pinned host tier, 1920x1080, orbit r=3000 at 1.2 deg/frame from a cold cache",
                gen="blobs", seed=2048, n=2048, iso=0.6, levelC=7, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
                dist=50.0, resident=0, l2flush=False, orbit=(3000.0, 1.2), dev_bytes=4 << 30,
-               host_bytes=16 << 30),
+               host_bytes=16 << 30, blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05)),
+    # profiling-sized version of c2 (1 GB volume) for ncu captures
+    "c2s": dict(workload="1024^3 f32 blobs+noise (c2 scaled by 1/2), iso 0.6, 16^3 bricks, 1920x1080, orbit r=1500",
+                gen="blobs", seed=2048, n=1024, iso=0.6, levelC=6, levelO=8, inc=3, W=1920, H=1080, fov=30.0,
+                dist=50.0, resident=0, l2flush=False, orbit=(1500.0, 1.2), dev_bytes=2 << 30,
+                host_bytes=4 << 30, blobs=(256, 10.0, 60.0, 0.5, 1.5, 0.05)),
+}
+
+# renderer modes: "plain" = the reference's scheme (one view per launch,
+# demand LRU from a cold cache); "best" = persistent ray queue + lookahead
+# requests (the product's default for the fly-through)
+MODES = {
+    "plain": dict(persistent=0, lookahead=0, use_graph=0),
+    "best": dict(persistent=1, lookahead=2, use_graph=1, pops=8, blocks_per_sm=8),
 }
 
 
@@ -86,7 +100,7 @@ class Clocks:
         sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows if len(r) >= 9 for i in range(4) if "Active" in r[5 + i]})
+        reasons = sorted({names[i] for r in rows if len(r) >= 9 for i in range(4) if r[5 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 
@@ -122,7 +136,7 @@ def frame_camera(vt, cfg, frame):
 class Workload:
     """Volume (device generated), octree (GPU builder) and renderer."""
 
-    def __init__(self, cfg, torch, device, workdir, need_renderer=True, host_copy=False):
+    def __init__(self, cfg, torch, device, workdir, need_renderer=True, mode="best"):
         import visualtur_b200 as vt
         self.vt, self.cfg = vt, cfg
         n = cfg["n"]
@@ -132,15 +146,14 @@ class Workload:
             c = (n - 1) / 2.0
             vt.generate_volume(vt.VT_GEN_SPHERE, cfg["seed"], (n, n, n), (c, c, c, 0.25), device_ptr=dvol.data_ptr())
         else:
-            vt.generate_volume(vt.VT_GEN_BLOBS, cfg["seed"], (n, n, n), (256, 20.0, 120.0, 0.5, 1.5, 0.05),
-                               device_ptr=dvol.data_ptr())
+            vt.generate_volume(vt.VT_GEN_BLOBS, cfg["seed"], (n, n, n), cfg["blobs"], device_ptr=dvol.data_ptr())
         torch.cuda.synchronize()
         t1 = time.time()
         self.octree_path = os.path.join(workdir, "vol_%s.oct" % cfg["gen"])
         vt.build_octree_device(dvol.data_ptr(), vt.VT_F32, (n, n, n), cfg["iso"], self.octree_path)
         t2 = time.time()
         # host copy of the volume: the out-of-core source and the CPU baseline's input
-        self.host = torch.empty(n * n * n, dtype=torch.float32, pin_memory=True)
+        self.host = torch.empty(n * n * n, dtype=torch.float32)
         self.host.copy_(dvol)
         torch.cuda.synchronize()
         del dvol
@@ -161,10 +174,17 @@ class Workload:
             p = vt.make_params(W=cfg["W"], H=cfg["H"], octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"],
                                levelCubes=cfg["levelC"], dimCube=edge, cubeInc=cfg["inc"], distance=cfg["dist"],
                                fov_H=cfg["fov"], fov_W=cfg["fov"], maxElementsCache=dev, maxElementsCache_CPU=host)
-            opt = vt.default_options(resident=cfg["resident"], record_hits=0, host_threads=0)
+            self.params = p
             t4 = time.time()
-            self.r = vt.visualTur(p, opt, volume=self.fm, octree=self.oc)
+            self.r = self.renderer(mode)
             log("setup: renderer %.1fs (device slots %d, host slots %d, %d B/brick)" % (time.time() - t4, dev, host, slot))
+
+
+    def renderer(self, mode):
+        """A renderer in `mode` (cold cache unless the workload is resident)."""
+        opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=0,
+                                      preload=1 if self.cfg["resident"] else 0, **MODES[mode])
+        return self.vt.visualTur(self.params, opt, volume=self.fm, octree=self.oc)
 
 
 def roofline(stats_frames, trace_ms, pixels):
@@ -221,95 +241,121 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, frame=0):
 
 
 # ----------------------------------------------------------------------------- arms
-def run_ours(args, cfg, rank, world, torch, dist):
-    vt_dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
-    torch.cuda.set_device(vt_dev)
-    work = tempfile.mkdtemp(prefix="vtbench_")
-    wl = Workload(cfg, torch, vt_dev, work)
-    r = wl.r
-    stream = torch.cuda.current_stream()
-    sp = stream.cuda_stream
+def timed_frames(wl, r, cfg, torch, dev, stream, frame0, warmup, steps, dist, clocks=None):
+    """Renders warmup + steps consecutive frames; returns per-frame device ms
+    (CUDA events on the launching stream) and per-frame stats."""
     W, H = cfg["W"], cfg["H"]
-    rgba = torch.empty(W * H * 4, dtype=torch.float32, device=vt_dev)
-    rgb8 = torch.empty(W * H * 3, dtype=torch.uint8, device=vt_dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=vt_dev) if cfg["l2flush"] else None
-    frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
-    for i in range(args.warmup):
-        r.set_camera(frame_camera(wl.vt, cfg, frame0 + i))
-        r.updateVisibleCubes(rgba, rgb8, stream=sp)
-    torch.cuda.synchronize()
-    r.reset_stats()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks = Clocks(vt_dev.index)
-    per_frame = []
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    for i in range(args.steps):
-        if flush is not None:
-            flush.zero_()
-        r.set_camera(frame_camera(wl.vt, cfg, frame0 + args.warmup + i))
-        ev[i][0].record(stream)
-        r.updateVisibleCubes(rgba, rgb8, stream=sp)
-        ev[i][1].record(stream)
-        per_frame.append(r.stats())
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = [a.elapsed_time(b) for a, b in ev]
-    tot_ms = sum(ms)
-    st = r.stats()
-    trace_ms = st["ms_trace_last_frame"]
-    # per-frame trace time: stats are cumulative except the last-frame fields
-    trace_tot = 0.0
-    prev = None
-    frames_stats = []
+    sp = stream.cuda_stream
+    rgba = torch.empty(W * H * 4, dtype=torch.float32, device=dev)
+    rgb8 = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if cfg["l2flush"] else None
+    with torch.cuda.stream(stream):
+        for i in range(warmup):
+            r.set_camera(frame_camera(wl.vt, cfg, frame0 + i))
+            r.updateVisibleCubes(rgba, rgb8, stream=sp)
+        torch.cuda.synchronize()
+        r.reset_stats()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        per_frame = []
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        for i in range(steps):
+            if flush is not None:
+                flush.zero_()
+            r.set_camera(frame_camera(wl.vt, cfg, frame0 + warmup + i))
+            ev[i][0].record(stream)
+            r.updateVisibleCubes(rgba, rgb8, stream=sp)
+            ev[i][1].record(stream)
+            per_frame.append(r.stats())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    clk = clocks.stop() if clocks else None
+    return [a.elapsed_time(b) for a, b in ev], per_frame, clk
+
+
+def frame_deltas(per_frame):
+    out, prev = [], None
     for s in per_frame:
-        trace_tot += s["ms_trace_last_frame"]
-        d = dict(s) if prev is None else {k: s[k] - prev[k] if isinstance(s[k], int) else s[k] for k in s}
-        frames_stats.append(d)
+        out.append(dict(s) if prev is None else {k: (s[k] - prev[k]) if isinstance(s[k], int) else s[k] for k in s})
         prev = s
+    return out
+
+
+def run_ours(args, cfg, rank, world, torch, dist):
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    work = tempfile.mkdtemp(prefix="vtbench_")
+    wl = Workload(cfg, torch, dev, work, mode=args.mode)
+    W, H = cfg["W"], cfg["H"]
+    stream = torch.cuda.Stream(device=dev)
+    frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
+    ms, per_frame, clk = timed_frames(wl, wl.r, cfg, torch, dev, stream, frame0, args.warmup, args.steps, dist,
+                                      Clocks(dev.index))
+    tot_ms = sum(ms)
+    st = wl.r.stats()
+    fd = frame_deltas(per_frame)
+    trace_tot = sum(s["ms_trace_last_frame"] for s in per_frame)
     rays_rank = W * H * args.steps
     t_max = tot_ms
     if dist:
-        t = torch.tensor([tot_ms], device=vt_dev)
+        t = torch.tensor([tot_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = rays_rank * world / (t_max * 1e-3)
     # end to end: public API with host output buffers (pose in, RGB8 image out)
-    e2e_steps = max(2, min(args.steps, 10))
-    out8 = np.empty((W * H, 3), np.uint8)
     import ctypes
+    e2e_steps = max(2, min(args.steps, 30))
+    out8 = np.empty((W * H, 3), np.uint8)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(e2e_steps):
-        r.set_camera(frame_camera(wl.vt, cfg, frame0 + args.warmup + args.steps + i))
-        wl.vt.check(wl.vt.lib().vt_render_host(r._h, None, out8.ctypes.data))
+        wl.r.set_camera(frame_camera(wl.vt, cfg, frame0 + args.warmup + args.steps + i))
+        wl.vt.check(wl.vt.lib().vt_render_host(wl.r._h, None, out8.ctypes.data))
     e2e_s = time.perf_counter() - t0
     e2e = {"value": round(W * H * e2e_steps / e2e_s * world, 1), "unit": "rays/s",
            "h2d_bytes_per_step": ctypes.sizeof(wl.vt.vt_camera), "d2h_bytes_per_step": W * H * 3,
-           "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3)}
+           "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3), "steps": e2e_steps,
+           "note": "continues the fly-through after the timed frames; wall clock around the synchronous host API"}
+    # the plain LRU renderer on the same frames, for comparison
+    plain = None
+    if args.mode != "plain" and not cfg["resident"] and not args.no_plain:
+        wl.r.close()
+        rp = wl.renderer("plain")
+        pms, pper, _ = timed_frames(wl, rp, cfg, torch, dev, stream, frame0, args.warmup, args.steps, dist)
+        plain = {"value": round(rays_rank * world / (sum(pms) * 1e-3), 1), "unit": "rays/s",
+                 "ms_per_step": round(sum(pms) / args.steps, 4),
+                 "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in pper) / args.steps, 4),
+                 "passes_per_step": round(sum(s["passes"] for s in pper) / args.steps, 3)}
+        rp.close()
     if rank != 0:
         return None
     line = {
-        "metric": "rays/s & ms/frame on 1 B200 (plain LRU renderer, single view)" if cfg["orbit"] else
-                  "rays/s & ms/frame on 1 B200 (resident march)",
+        "metric": "rays/s & ms/frame on 1 B200 (%s)" % ("resident march" if cfg["resident"] else
+                                                         "out-of-core fly-through, %s renderer" % args.mode),
         "value": round(value, 1), "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, device-generated)",
-        "config": {"workload": cfg["workload"], "name": args.config, "W": W, "H": H,
+        "config": {"workload": cfg["workload"], "name": args.config, "mode": args.mode, "W": W, "H": H,
                    "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": roofline(frames_stats, trace_tot, W * H * args.steps),
+        "roofline": roofline(fd, trace_tot, W * H * args.steps),
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": int(st["launches"]),
-        "frame_stats": {k: st[k] for k in ("passes", "bricks_requested", "bricks_loaded_disk", "host_hits",
-                                           "device_hits", "device_misses", "hits", "samples", "candidates")},
-        "ms_trace_total": round(trace_tot, 3),
+        "frame_stats": {"passes_per_step": round(sum(s["passes"] for s in per_frame) / args.steps, 3),
+                        "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in per_frame) / args.steps, 4),
+                        "trace_ms_per_step": round(trace_tot / args.steps, 4),
+                        "bricks_requested": st["bricks_requested"], "bricks_loaded_disk": st["bricks_loaded_disk"],
+                        "device_hits": st["device_hits"], "device_misses": st["device_misses"],
+                        "hits": st["hits"], "samples": st["samples"], "candidates": st["candidates"],
+                        "expansions": st["expansions"]},
     }
+    if plain:
+        line["plain_lru"] = plain
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, frame=frame0 + args.warmup)
     return line
@@ -347,13 +393,15 @@ def run_reference(args, cfg, rank, world, torch):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default=os.environ.get("VT_BENCH_CONFIG", "c2"), choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--ref-budget", type=float, default=6.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="best", choices=sorted(MODES))
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-LRU comparison run")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -368,6 +416,8 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = tdist
     cfg = CONFIGS[args.config]
+    if args.steps is None:
+        args.steps = 300 if cfg["orbit"] else 200     # c2: the 300-frame orbit
     if args.impl == "reference":
         line = run_reference(args, cfg, rank, world, torch)
     else:

@@ -164,6 +164,11 @@ typedef struct {
     int record_trace;      /* log per-frame touched coarse nodes */
     int trace_level;       /* octree level of the logged nodes (4 in C4) */
     int record_hits;       /* keep per-ray hit node/brick/t/normal for vt_debug_hits */
+    int persistent;        /* 1: persistent ray-queue kernel with warp refill */
+    int blocks_per_sm;     /* persistent grid: CTAs per SM (autotuned) */
+    int pops;              /* persistent: traversal steps between warp refills */
+    int preload;           /* 1: load every needed brick at create when they fit */
+    int use_graph;         /* 1: pass 0 of a frame replays a captured CUDA graph */
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -201,6 +206,20 @@ typedef struct {
     uint8_t* dev_rgb8;      /* W*H*3 bytes, may be NULL */
 } vt_view;
 vt_status vt_render_batch(vt_handle* h, const vt_view* views, int n, void* stream);
+
+/* Coarse-node access trace of the last frame (record_trace): bit k of
+ * `bits` = node 8^trace_level + k was marched.  nwords = 8^trace_level/32;
+ * the call synchronises. */
+vt_status vt_get_trace(vt_handle* h, uint32_t* bits, int64_t nwords);
+
+/* Loads the given bricks (codes at levelCubes) into the device cache ahead
+ * of demand, on `stream`; bricks used by the current frame are never
+ * evicted.  Returns the number loaded in *loaded (may be NULL). */
+vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n, int64_t* loaded, void* stream);
+
+/* Bricks (codes at levelCubes) that hold candidate nodes of the octree,
+ * sorted; n in/out: capacity / count. */
+vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n);
 
 /* Per-ray diagnostics of the last vt_render (host buffers, W*H entries,
  * any may be NULL): hit node Morton code at octreeLevel (0 = none), brick

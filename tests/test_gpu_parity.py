@@ -30,9 +30,11 @@ def product_render(case, workdir, mode, vol=None, extra_ops=()):
     oc = vt.Octree(F.case_octree(case, workdir))
     nb = 8 ** c["levelC"]
     dev, host = nb, nb
-    if mode == "demand":
+    if mode.startswith("demand"):
         dev, host = 24, 16
-    opt = vt.default_options(resident=1 if mode == "resident" else 0, record_hits=1)
+    opt = vt.default_options(resident=1 if mode in ("resident", "persist") else 0, record_hits=1,
+                             persistent=1 if mode in ("persist", "demand_la") else 0,
+                             lookahead=3 if mode == "demand_la" else 0, pops=3)
     p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=c["levelO"],
                        levelCubes=c["levelC"], dimCube=1 << (int(np.log2(c["n"])) - c["levelC"]),
                        cubeInc=c["inc"], distance=c["dist"], fov_H=c["fov"], fov_W=c["fov"],
@@ -71,7 +73,7 @@ def assert_parity(a, b):
     assert np.array_equal(a["rgb8"], b["rgb8"])
 
 
-@pytest.mark.parametrize("mode", ["resident", "slab", "demand"])
+@pytest.mark.parametrize("mode", ["resident", "slab", "demand", "persist", "demand_la"])
 @pytest.mark.parametrize("case", sorted(F.CASES))
 def test_render_parity(case, mode, workdir, cuda):
     a = product_render(case, workdir, mode)
@@ -80,7 +82,7 @@ def test_render_parity(case, mode, workdir, cuda):
     assert a["stats"]["hits"] == b["agg"]["hits"]
     assert a["stats"]["samples"] == b["agg"]["samples"]
     assert a["stats"]["candidates"] == b["agg"]["candidates"]
-    if mode == "demand":
+    if mode.startswith("demand"):
         assert a["stats"]["passes"] > 1 and a["stats"]["bricks_requested"] > 24
 
 
@@ -153,3 +155,86 @@ def test_render_into_device_buffers_and_repeat(workdir, cuda):
     assert np.array_equal(outs[0][1].reshape(-1, 3), exp["rgb8"])
     st = r.stats()
     assert st["frames"] == 3 and st["passes"] == 1
+
+
+def _views(vt_, torch, cams):
+    views, bufs = [], []
+    for cam in cams:
+        n = cam.W * cam.H
+        rgba = torch.empty(n * 4, dtype=torch.float32, device="cuda")
+        rgb8 = torch.empty(n * 3, dtype=torch.uint8, device="cuda")
+        v = vt.vt_view()
+        v.cam = cam
+        v.dev_rgba, v.dev_rgb8 = rgba.data_ptr(), rgb8.data_ptr()
+        views.append(v)
+        bufs.append((rgba, rgb8))
+    return views, bufs
+
+
+BATCH = [((96, 96), [("mv", (31.5, 31.5, 181.5))]),
+         ((50, 37), [("mv", (31.5, 31.5, 181.5)), ("ry", 20.0), ("mf", 30.0)]),
+         ((128, 72), [("mv", (31.5, 31.5, 181.5)), ("rx", -12.0), ("rz", 33.0), ("sr", 4.0)]),
+         ((33, 65), [("mv", (-80.0, 40.0, 31.5)), ("ry", -90.0)])]
+
+
+@pytest.mark.parametrize("mode", ["resident", "demand", "persist", "demand_la"])
+def test_batch_parity(mode, workdir, cuda):
+    """Several views of different sizes in one launch equal per-view oracle renders."""
+    torch = cuda
+    c = F.CASES["s64"]
+    fm, oc = vt.FileManager.wrap(F.case_volume("s64")), vt.Octree(F.case_octree("s64", workdir))
+    dev, host = (24, 16) if mode.startswith("demand") else (512, 512)
+    opt = vt.default_options(resident=1 if mode in ("resident", "persist") else 0, record_hits=0,
+                             persistent=1 if mode in ("persist", "demand_la") else 0,
+                             lookahead=2 if mode == "demand_la" else 0, pops=2, tile_w=4, tile_h=4)
+    p = vt.make_params(W=96, H=96, octreeFile=None, hdf5File=None, octreeLevel=4, levelCubes=3, dimCube=8,
+                       distance=50.0, fov_H=30.0, fov_W=30.0, maxElementsCache=dev, maxElementsCache_CPU=host)
+    r = vt.visualTur(p, opt, volume=fm, octree=oc)
+    cams = []
+    for (W, H), ops in BATCH:
+        cam = vt.Camera(H, W, 50.0, 30.0, 27.0)
+        for op, v in ops:
+            {"mv": cam.Move, "rx": cam.RotateX, "ry": cam.RotateY, "rz": cam.RotateZ, "mf": cam.MoveForward,
+             "sr": cam.StrafeRight}[op](v)
+        cams.append(cam)
+    views, bufs = _views(vt, torch, [cm.c for cm in cams])
+    r.render_batch(views)
+    torch.cuda.synchronize()
+    o = orc.Octree(F.case_octree("s64", workdir))
+    vol = F.case_volume("s64")
+    for ((W, H), ops), (rgba, rgb8) in zip(BATCH, bufs):
+        ocam = orc.Camera(H, W, 50.0, 30.0, 27.0)
+        orc.apply_ops(ocam, ops)
+        exp = orc.render(o, vol, ocam, c["levelO"], c["levelC"], c["inc"])
+        assert np.array_equal(rgba.cpu().numpy().reshape(-1, 4).view(np.uint32), exp["rgba"].view(np.uint32))
+        assert np.array_equal(rgb8.cpu().numpy().reshape(-1, 3), exp["rgb8"])
+    if mode.startswith("demand"):
+        assert r.stats()["passes"] > 1
+
+
+def test_trace_log_and_prefetch(workdir, cuda):
+    c = F.CASES["c1"]
+    fm, oc = vt.FileManager.wrap(F.case_volume("c1")), vt.Octree(F.case_octree("c1", workdir))
+    opt = vt.default_options(resident=0, preload=0, record_trace=1, trace_level=2, record_hits=1)
+    p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=5, levelCubes=4, dimCube=8,
+                       distance=50.0, fov_H=30.0, fov_W=30.0, maxElementsCache=4096, maxElementsCache_CPU=4096)
+    r = vt.visualTur(p, opt, volume=fm, octree=oc)
+    r.camera_Move((63.5, 63.5, 363.5))
+    rgba1, _ = r.render_host(rgb8=False)
+    st1 = r.stats()
+    assert st1["passes"] > 1                       # cold cache: demand passes
+    node = r.debug_hits()[0]
+    bits = r.trace(2)
+    touched = {64 + k for k in range(64) if (bits[k // 32] >> (k % 32)) & 1}
+    hit_anc = {int(n) >> 9 for n in node[node != 0]}     # level-5 code -> level-2 ancestor
+    assert hit_anc and hit_anc <= touched
+    # second frame of the same pose: every brick now resident, one pass
+    r.reset_stats()
+    rgba2, _ = r.render_host(rgb8=False)
+    assert r.stats()["passes"] == 1 and np.array_equal(rgba1, rgba2)
+    # a fresh cold handle with every brick prefetched renders in one pass
+    r2 = vt.visualTur(p, vt.default_options(resident=0, preload=0), volume=fm, octree=oc)
+    r2.camera_Move((63.5, 63.5, 363.5))
+    assert r2.prefetch(r2.brick_list()) > 0
+    rgba3, _ = r2.render_host(rgb8=False)
+    assert r2.stats()["passes"] == 1 and np.array_equal(rgba1, rgba3)

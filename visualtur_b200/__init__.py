@@ -45,7 +45,8 @@ class vt_params(C.Structure):
 
 class vt_options(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("resident", "tile_w", "tile_h", "unroll", "lookahead", "max_passes",
-                                         "host_threads", "record_trace", "trace_level", "record_hits")]
+                                         "host_threads", "record_trace", "trace_level", "record_hits",
+                                         "persistent", "blocks_per_sm", "pops", "preload", "use_graph")]
 
 
 class vt_stats(C.Structure):
@@ -104,6 +105,9 @@ _PROTOS = {
     "vt_render_host": (C.c_int, [_P, _P, _P]),
     "vt_render_batch": (C.c_int, [_P, C.POINTER(vt_view), C.c_int, _P]),
     "vt_debug_hits": (C.c_int, [_P, _P, _P, _P, _P]),
+    "vt_get_trace": (C.c_int, [_P, _P, C.c_int64]),
+    "vt_prefetch": (C.c_int, [_P, _P, C.c_int64, C.POINTER(C.c_int64), _P]),
+    "vt_brick_list": (C.c_int, [_P, _P, C.POINTER(C.c_int64)]),
     "vt_get_stats": (C.c_int, [_P, C.POINTER(vt_stats)]),
     "vt_reset_stats": (C.c_int, [_P]),
 }
@@ -421,6 +425,25 @@ class visualTur:
         nrm = np.empty((n, 3), np.float32)
         check(lib().vt_debug_hits(self._h, node.ctypes.data, brick.ctypes.data, t.ctypes.data, nrm.ctypes.data))
         return node, brick, t, nrm
+
+    def trace(self, level=4):
+        nw = max(1, (8 ** level) // 32)
+        out = np.empty(nw, np.uint32)
+        check(lib().vt_get_trace(self._h, out.ctypes.data, nw))
+        return out
+
+    def prefetch(self, bricks, stream=None):
+        b = np.ascontiguousarray(bricks, np.uint64)
+        got = C.c_int64()
+        check(lib().vt_prefetch(self._h, b.ctypes.data, int(b.size), C.byref(got), stream))
+        return got.value
+
+    def brick_list(self):
+        n = C.c_int64(0)
+        check(lib().vt_brick_list(self._h, None, C.byref(n)))
+        out = np.empty(n.value, np.uint64)
+        check(lib().vt_brick_list(self._h, out.ctypes.data, C.byref(n)))
+        return out
 
     def stats(self):
         s = vt_stats()

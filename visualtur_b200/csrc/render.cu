@@ -128,52 +128,74 @@ __device__ __forceinline__ void setup_sampler(const TraceArgs& A, unsigned long 
     }
 }
 
-struct RayOut {
-    float4 rgba; unsigned long long node, brick; float t; float3 n; bool hit;
+/* One ray in flight. */
+struct Ray {
+    RayInv r;
+    float3 dir;
+    int top;
+    int view, i, j;
+    unsigned int g;        /* padded global ray index */
+    float4 rgba;
+    unsigned long long node, brick;
+    float t;
+    float3 n;
+    bool hit;
 };
 
-/* Runs one ray's DFS from its stack until it finishes (returns true) or
- * suspends on an absent brick (returns false; stack holds the state). */
+enum { RAY_RUNNING = 0, RAY_DONE = 1, RAY_SUSPENDED = 2 };
+
+/* requests brick `brick` once per pass (page -1 -> -2) */
+__device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned long long brick) {
+    int old = atomicCAS(&A.br.page[brick - A.br.pageBase], -1, -2);
+    if (old == -1) {
+        unsigned int q = atomicAdd(A.ctl.n_req, 1u);
+        if (q < A.ctl.req_cap) A.ctl.req[q] = brick;
+        else atomicOr(A.ctl.err, VT_KERR_REQUEST_FULL);
+    }
+}
+
+/* Advances one ray's DFS by at most `budget` pops (src/Octree.cu:620-720
+ * interleaved with src/rayCaster.cu:139-265).  Returns RAY_DONE when the
+ * ray is shaded or exhausted, RAY_SUSPENDED when its next candidate's brick
+ * is not resident (the candidate stays on the stack), RAY_RUNNING when the
+ * budget ran out. */
 template <int VTYPE, bool SLAB>
-__device__ bool trace_ray(const TraceArgs& A, const RayInv& r, float3 dir, Stk& st, int& top,
-                          RayOut& o, unsigned int* cnt) {
+__device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, int budget) {
     const DevOctree& O = A.oct;
     const int nLevels = O.nLevels, Lo = O.Lo;
     const int codeBits = 3 * Lo + 1;
     const unsigned long long codeMask = (1ull << codeBits) - 1ull;
     const int dimO = 1 << (nLevels - Lo);
     const int shiftOC = 3 * (Lo - O.Lc);
-    while (top >= 0) {
-        unsigned long long ent = st.e[top];
+    while (R.top >= 0) {
+        if (budget-- == 0) return RAY_RUNNING;
+        unsigned long long ent = st.e[R.top];
         unsigned long long code = ent & codeMask;
         unsigned int idx = (unsigned int)(ent >> codeBits);
         int level = code_level(code);
         int3 mb = min_box(code, level, nLevels);
         if (level == Lo) {
-            /* candidate: brick lookup (lruCache::updateCube :177-291) */
+            /* candidate: brick lookup (lruCache::updateCube, src/lruCache.cu:177-291) */
             unsigned long long brick = code >> shiftOC;
             Samp s; int slot;
             setup_sampler<VTYPE, SLAB>(A, brick, s, &slot);
             if (SLAB && slot < 0) {
-                if (slot == -1) {
-                    int old = atomicCAS(&A.br.page[brick - A.br.pageBase], -1, -2);
-                    if (old == -1) {
-                        unsigned int q = atomicAdd(A.ctl.n_req, 1u);
-                        if (q < A.ctl.req_cap) A.ctl.req[q] = brick;
-                        else atomicOr(A.ctl.err, VT_KERR_REQUEST_FULL);
-                    }
-                }
+                if (slot == -1) request_brick(A, brick);
                 cnt[VT_C_DEVMISSES]++;
-                return false;   /* suspend with the candidate still on top */
+                return RAY_SUSPENDED;
             }
-            top--;
+            R.top--;
             cnt[VT_C_CANDIDATES]++;
             if (SLAB) { cnt[VT_C_DEVHITS]++; A.br.stamp[slot] = A.br.pass; }
+            if (A.ctl.touched) {
+                unsigned long long tn = (code >> A.ctl.touch_shift) - A.ctl.touch_base;
+                atomicOr(&A.ctl.touched[tn >> 5], 1u << (tn & 31));
+            }
             float tn, tf;
-            if (!slab(r, mb.x, mb.y, mb.z, mb.x + dimO, mb.y + dimO, mb.z + dimO, &tn, &tf)) continue;
+            if (!slab(R.r, mb.x, mb.y, mb.z, mb.x + dimO, mb.y + dimO, mb.z + dimO, &tn, &tf)) continue;
             float3 X;
             unsigned int ns = 0;
-            bool h = march<VTYPE>(s, r.o, dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
+            bool h = march<VTYPE>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
             cnt[VT_C_SAMPLES] += ns;
             if (h) {
                 /* shade (src/rayCaster.cu:238-250) */
@@ -182,16 +204,16 @@ __device__ bool trace_ray(const TraceArgs& A, const RayInv& r, float3 dir, Stk& 
                 float3 l = normalize(sub(X, A.light));
                 float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
                 float a = X.y / 256.0f;
-                o.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
-                o.hit = true; o.node = code; o.brick = brick; o.n = n;
-                o.t = dot(sub(X, r.o), dir);
-                return true;
+                R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
+                R.hit = true; R.node = code; R.brick = brick; R.n = n;
+                R.t = dot(sub(X, R.r.o), R.dir);
+                return RAY_DONE;
             }
             continue;
         }
         /* expansion: _cuda_searchChildrenValidAndHit2 (src/Octree.cu:375-532)
          * with membership from the flattened child mask */
-        top--;
+        R.top--;
         cnt[VT_C_EXPANSIONS]++;
         uint2 nd = O.nodes[level][idx];
         const int cl = level + 1;
@@ -205,7 +227,7 @@ __device__ bool trace_ray(const TraceArgs& A, const RayInv& r, float3 dir, Stk& 
             if ((m >> k) & 1u) {
                 int bx = mb.x + ((k >> 2) & 1) * cd, by = mb.y + ((k >> 1) & 1) * cd, bz = mb.z + (k & 1) * cd;
                 float a, b;
-                if (slab(r, bx, by, bz, bx + cd, by + cd, bz + cd, &a, &b) && b >= 0.0f) {
+                if (slab(R.r, bx, by, bz, bx + cd, by + cd, bz + cd, &a, &b) && b >= 0.0f) {
                     unsigned long long cidx = nd.x + __popc(m & ((1u << k) - 1u));
                     cent[nv] = (cidx << codeBits) | ((code << 3) + (unsigned long long)k);
                     ctn[nv] = a; ctf[nv] = b;
@@ -217,100 +239,162 @@ __device__ bool trace_ray(const TraceArgs& A, const RayInv& r, float3 dir, Stk& 
         int n = nv;
         while (n != 0) {
             int newn = 0;
-            for (int i = 1; i < nv; i++) {
-                if (ctn[i - 1] > ctn[i] || (ctn[i - 1] == ctn[i] && ctf[i - 1] > ctf[i])) {
-                    unsigned long long te = cent[i]; cent[i] = cent[i - 1]; cent[i - 1] = te;
-                    float tt = ctn[i]; ctn[i] = ctn[i - 1]; ctn[i - 1] = tt;
-                    tt = ctf[i]; ctf[i] = ctf[i - 1]; ctf[i - 1] = tt;
-                    newn = i;
+            for (int q = 1; q < nv; q++) {
+                if (ctn[q - 1] > ctn[q] || (ctn[q - 1] == ctn[q] && ctf[q - 1] > ctf[q])) {
+                    unsigned long long te = cent[q]; cent[q] = cent[q - 1]; cent[q - 1] = te;
+                    float tt = ctn[q]; ctn[q] = ctn[q - 1]; ctn[q - 1] = tt;
+                    tt = ctf[q]; ctf[q] = ctf[q - 1]; ctf[q - 1] = tt;
+                    newn = q;
                 }
             }
             n = newn;
         }
-        if (top + nv >= VT_STACK) {
+        if (R.top + nv >= VT_STACK) {
             atomicOr(A.ctl.err, VT_KERR_STACK);
-            top = -1;
-            break;
+            R.top = -1;
+            return RAY_DONE;
         }
-        for (int i = nv - 1; i >= 0; i--) st.e[++top] = cent[i];
-        if ((unsigned int)(top + 1) > cnt[VT_C_MAXSTACK]) cnt[VT_C_MAXSTACK] = top + 1;
+        for (int q = nv - 1; q >= 0; q--) st.e[++R.top] = cent[q];
+        if ((unsigned int)(R.top + 1) > cnt[VT_C_MAXSTACK]) cnt[VT_C_MAXSTACK] = R.top + 1;
     }
-    return true;   /* exhausted: background */
+    return RAY_DONE;   /* exhausted: background */
+}
+
+/* Speculative requests: walks a copy of a suspended ray's DFS (without
+ * marching) and requests up to `lookahead` further absent bricks. */
+template <int VTYPE>
+__device__ void lookahead_requests(const TraceArgs& A, Ray R, Stk& st) {
+    const DevOctree& O = A.oct;
+    const int nLevels = O.nLevels, Lo = O.Lo;
+    const int codeBits = 3 * Lo + 1;
+    const unsigned long long codeMask = (1ull << codeBits) - 1ull;
+    const int shiftOC = 3 * (Lo - O.Lc);
+    int want = A.ctl.lookahead, pops = 0;
+    unsigned long long last = 0;
+    while (R.top >= 0 && want > 0 && pops++ < 256) {
+        unsigned long long ent = st.e[R.top--];
+        unsigned long long code = ent & codeMask;
+        unsigned int idx = (unsigned int)(ent >> codeBits);
+        int level = code_level(code);
+        if (level == Lo) {
+            unsigned long long brick = code >> shiftOC;
+            if (brick != last && A.br.page[brick - A.br.pageBase] == -1) { request_brick(A, brick); want--; }
+            last = brick;
+            continue;
+        }
+        int3 mb = min_box(code, level, nLevels);
+        uint2 nd = O.nodes[level][idx];
+        const int cd = 1 << (nLevels - level - 1);
+        unsigned long long cent[8];
+        float ctn[8];
+        int nv = 0;
+        for (int k = 0; k < 8; k++) {
+            if ((nd.y >> k) & 1u) {
+                int bx = mb.x + ((k >> 2) & 1) * cd, by = mb.y + ((k >> 1) & 1) * cd, bz = mb.z + (k & 1) * cd;
+                float a, b;
+                if (slab(R.r, bx, by, bz, bx + cd, by + cd, bz + cd, &a, &b) && b >= 0.0f) {
+                    cent[nv] = ((unsigned long long)(nd.x + __popc(nd.y & ((1u << k) - 1u))) << codeBits) |
+                               ((code << 3) + (unsigned long long)k);
+                    ctn[nv++] = a;
+                }
+            }
+        }
+        for (int q = 1; q < nv; q++)      /* near first (order only affects which bricks get asked) */
+            for (int p = q; p > 0 && ctn[p - 1] > ctn[p]; p--) {
+                float tt = ctn[p]; ctn[p] = ctn[p - 1]; ctn[p - 1] = tt;
+                unsigned long long te = cent[p]; cent[p] = cent[p - 1]; cent[p - 1] = te;
+            }
+        if (R.top + nv >= VT_STACK) break;
+        for (int q = nv - 1; q >= 0; q--) st.e[++R.top] = cent[q];
+    }
+}
+
+/* padded global ray index -> view and pixel (tile order) */
+__device__ __forceinline__ bool decode_ray(const DevView* sv, int nv, int tw, int th, unsigned int g, int& v, int& i,
+                                           int& j) {
+    v = 0;
+    for (int k = 1; k < nv; k++) if (sv[k].rayBase <= g) v = k;
+    unsigned int local = g - sv[v].rayBase;
+    unsigned int tile = local / (unsigned)(tw * th), lt = local % (unsigned)(tw * th);
+    unsigned int ti = tile / sv[v].tilesX, tj = tile % sv[v].tilesX;
+    i = (int)(ti * th + lt / tw);
+    j = (int)(tj * tw + lt % tw);
+    return i < sv[v].cam.H && j < sv[v].cam.W;
+}
+
+/* Sets up work item w (pass 0: padded ray index; later passes: suspended
+ * record).  Returns RAY_RUNNING when the ray has traversal to do, RAY_DONE
+ * when it is background already (root miss), -1 for tile padding. */
+template <int VTYPE>
+__device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, Ray& R, Stk& st,
+                          unsigned int* cnt) {
+    unsigned int depth = 0;
+    unsigned long long off = 0;
+    bool resume = A.ctl.in != nullptr;
+    if (resume) {
+        SuspRec rec = A.ctl.in[w];
+        R.g = rec.ray; depth = rec.depth; off = rec.off;
+    } else {
+        R.g = w;
+    }
+    if (!decode_ray(sv, A.views.n, A.tile_w, A.tile_h, R.g, R.view, R.i, R.j)) return -1;
+    const DevCamera& C = sv[R.view].cam;
+    R.dir = ray_dir(C.look, C.up, C.right, C.dist, C.h, C.w, C.H, C.W, R.i, R.j);
+    R.r.o = C.pos; R.r.dx = 1 / R.dir.x; R.r.dy = 1 / R.dir.y; R.r.dz = 1 / R.dir.z;
+    R.rgba = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+    R.hit = false; R.node = 0; R.brick = 0; R.t = -1.0f; R.n = f3(0, 0, 0);
+    R.top = -1;
+    if (resume && depth > 0) {
+        R.top = (int)depth - 1;
+        for (int e = 0; e <= R.top; e++) st.e[e] = A.ctl.pool_in[off + e];
+        return RAY_RUNNING;
+    }
+    if (!resume) cnt[VT_C_RAYS]++;
+    const int N = 1 << A.oct.nLevels;
+    float tn, tf;
+    /* root test (src/Octree.cu:729) */
+    if (A.oct.rootValid && slab(R.r, 0, 0, 0, N, N, N, &tn, &tf)) { R.top = 0; st.e[0] = 1ull; return RAY_RUNNING; }
+    return RAY_DONE;   /* background */
+}
+
+__device__ __forceinline__ void write_ray(const TraceArgs& A, const DevView* sv, const Ray& R, unsigned int* cnt) {
+    const DevView& V = sv[R.view];
+    const size_t id = (size_t)R.i * V.cam.W + R.j;
+    if (R.hit) cnt[VT_C_HITS]++;
+    if (V.rgba) V.rgba[id] = R.rgba;
+    if (V.rgb8) {
+        V.rgb8[3 * id] = to_u8(R.rgba.x);
+        V.rgb8[3 * id + 1] = to_u8(R.rgba.y);
+        V.rgb8[3 * id + 2] = to_u8(R.rgba.z);
+    }
+    if (R.view == 0) {
+        if (A.out.node) A.out.node[id] = R.node;
+        if (A.out.brick) A.out.brick[id] = R.brick;
+        if (A.out.t) A.out.t[id] = R.t;
+        if (A.out.n) { A.out.n[3 * id] = R.n.x; A.out.n[3 * id + 1] = R.n.y; A.out.n[3 * id + 2] = R.n.z; }
+    }
 }
 
 template <int VTYPE, bool SLAB>
-__global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
-    unsigned int cnt[VT_C_COUNT];
-#pragma unroll
-    for (int c = 0; c < VT_C_COUNT; c++) cnt[c] = 0;
-    const DevCamera& C = A.cam;
-    int i = -1, j = -1, slotIn = -1;
-    if (A.ctl.susp_in == nullptr) {
-        int tw = A.tile_w, th = A.tile_h;
-        int tilesX = (C.W + tw - 1) / tw;
-        int tile = blockIdx.x * (blockDim.x / (tw * th)) + threadIdx.x / (tw * th);
-        int lt = threadIdx.x % (tw * th);
-        int ti = tile / tilesX, tj = tile % tilesX;
-        i = ti * th + lt / tw;
-        j = tj * tw + lt % tw;
-        if (i >= C.H || j >= C.W) i = -1;
+__device__ __forceinline__ void suspend_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt) {
+    cnt[VT_C_SUSPENDED]++;
+    unsigned int q = atomicAdd(A.ctl.n_out, 1u);
+    if (q >= A.ctl.out_cap) { atomicOr(A.ctl.err, VT_KERR_SUSPEND_FULL); return; }
+    unsigned int depth = (unsigned int)(R.top + 1);
+    unsigned long long off = atomicAdd(A.ctl.pool_used, (unsigned long long)depth);
+    SuspRec rec;
+    rec.ray = R.g;
+    if (off + depth <= A.ctl.pool_cap) {
+        for (unsigned int e = 0; e < depth; e++) A.ctl.pool_out[off + e] = st.e[e];
+        rec.depth = depth; rec.off = off;
     } else {
-        unsigned int t = blockIdx.x * blockDim.x + threadIdx.x;
-        if (t < A.ctl.n_in) {
-            unsigned int id = A.ctl.susp_in[t];
-            i = id / C.W; j = id % C.W; slotIn = (int)t;
-        }
+        rec.depth = 0; rec.off = 0;   /* pool full: the ray restarts from the root (same result) */
     }
-    if (i >= 0) {
-        const int id = i * C.W + j;
-        float3 dir = ray_dir(C.look, C.up, C.right, C.dist, C.h, C.w, C.H, C.W, i, j);
-        RayInv r;
-        r.o = C.pos; r.dx = 1 / dir.x; r.dy = 1 / dir.y; r.dz = 1 / dir.z;
-        RayOut o;
-        o.rgba = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        o.hit = false; o.node = 0; o.brick = 0; o.t = -1.0f; o.n = f3(0, 0, 0);
-        Stk st;
-        int top = -1;
-        bool start = true;
-        if (slotIn >= 0) {
-            top = (int)A.ctl.top_in[slotIn] - 1;
-            for (int e = 0; e <= top; e++) st.e[e] = A.ctl.stk_in[(size_t)slotIn * VT_STACK + e];
-            start = false;
-        } else {
-            cnt[VT_C_RAYS]++;
-            const int N = 1 << A.oct.nLevels;
-            float tn, tf;
-            /* root test (src/Octree.cu:729) */
-            if (A.oct.rootValid && slab(r, 0, 0, 0, N, N, N, &tn, &tf)) { top = 0; st.e[0] = 1ull; }
-        }
-        (void)start;
-        bool done = trace_ray<VTYPE, SLAB>(A, r, dir, st, top, o, cnt);
-        if (done) {
-            if (o.hit) cnt[VT_C_HITS]++;
-            if (A.out.rgba) A.out.rgba[id] = o.rgba;
-            if (A.out.rgb8) {
-                A.out.rgb8[3 * (size_t)id] = to_u8(o.rgba.x);
-                A.out.rgb8[3 * (size_t)id + 1] = to_u8(o.rgba.y);
-                A.out.rgb8[3 * (size_t)id + 2] = to_u8(o.rgba.z);
-            }
-            if (A.out.node) A.out.node[id] = o.node;
-            if (A.out.brick) A.out.brick[id] = o.brick;
-            if (A.out.t) A.out.t[id] = o.t;
-            if (A.out.n) { A.out.n[3 * (size_t)id] = o.n.x; A.out.n[3 * (size_t)id + 1] = o.n.y; A.out.n[3 * (size_t)id + 2] = o.n.z; }
-        } else {
-            unsigned int q = atomicAdd(A.ctl.n_out, 1u);
-            if (q < A.ctl.susp_cap) {
-                A.ctl.susp_out[q] = (unsigned int)id;
-                A.ctl.top_out[q] = (unsigned char)(top + 1);
-                unsigned long long* dst = A.ctl.stk_out + (size_t)q * VT_STACK;
-                for (int e = 0; e <= top; e++) dst[e] = st.e[e];
-            } else {
-                atomicOr(A.ctl.err, VT_KERR_SUSPEND_FULL);
-            }
-            cnt[VT_C_SUSPENDED]++;
-        }
-    }
-    /* warp-aggregated counters */
+    A.ctl.out[q] = rec;
+    if (SLAB && A.ctl.lookahead > 0) lookahead_requests<VTYPE>(A, R, st);
+}
+
+__device__ __forceinline__ void flush_counters(const TraceArgs& A, unsigned int* cnt) {
 #pragma unroll
     for (int c = 0; c < VT_C_COUNT; c++) {
         unsigned int v = cnt[c];
@@ -322,6 +406,59 @@ __global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
             if ((threadIdx.x & 31) == 0 && v) atomicAdd(&A.ctl.counters[c], (unsigned long long)v);
         }
     }
+}
+
+/* One ray per thread (PERSIST = false) or a persistent ray queue: each warp
+ * keeps its 32 lanes busy, and after every `pops` traversal steps the lanes
+ * whose ray finished or suspended take new work items -- a ballot of the
+ * idle lanes, one atomicAdd by the leader, and a popcount rank per lane. */
+template <int VTYPE, bool SLAB, bool PERSIST>
+__global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
+    __shared__ DevView sv[VT_MAX_VIEWS];
+    for (int k = threadIdx.x; k < A.views.n; k += blockDim.x) sv[k] = A.views.v[k];
+    __syncthreads();
+    unsigned int cnt[VT_C_COUNT];
+#pragma unroll
+    for (int c = 0; c < VT_C_COUNT; c++) cnt[c] = 0;
+    const unsigned int nItems = A.ctl.in ? A.ctl.n_in : A.views.totalRays;
+    Stk st;
+    Ray R;
+    if (!PERSIST) {
+        unsigned int w = blockIdx.x * blockDim.x + threadIdx.x;
+        if (w < nItems) {
+            int s = start_ray<VTYPE>(A, sv, w, R, st, cnt);
+            if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB>(A, R, st, cnt, -1);
+            if (s == RAY_DONE) write_ray(A, sv, R, cnt);
+            else if (s == RAY_SUSPENDED) suspend_ray<VTYPE, SLAB>(A, R, st, cnt);
+        }
+    } else {
+        const unsigned int lane = threadIdx.x & 31;
+        bool has = false;
+        for (;;) {
+            unsigned int need = __ballot_sync(0xffffffffu, !has);
+            if (need) {
+                unsigned int base = 0;
+                int leader = __ffs(need) - 1;
+                if ((int)lane == leader) base = atomicAdd(A.ctl.work, (unsigned int)__popc(need));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base >= nItems && need == 0xffffffffu) break;   /* queue drained, warp idle */
+                if (!has) {
+                    unsigned int w = base + __popc(need & ((1u << lane) - 1u));
+                    if (w < nItems) {
+                        int s = start_ray<VTYPE>(A, sv, w, R, st, cnt);
+                        has = s == RAY_RUNNING;
+                        if (s == RAY_DONE) write_ray(A, sv, R, cnt);
+                    }
+                }
+            }
+            if (has) {
+                int s = run_ray<VTYPE, SLAB>(A, R, st, cnt, A.pops);
+                if (s == RAY_DONE) { write_ray(A, sv, R, cnt); has = false; }
+                else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB>(A, R, st, cnt); has = false; }
+            }
+        }
+    }
+    flush_counters(A, cnt);
 }
 
 /* cuda_updateRays (src/Camera.cu:39-74) */
@@ -432,26 +569,31 @@ __global__ void k_fill_dense(void* dst, const void* src, long long nx, long long
 
 using namespace vt;
 
-cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, cudaStream_t s) {
+cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, bool persistent, int blocksPerSM, cudaStream_t s) {
     const int threads = 128;
+    unsigned int items = a.ctl.in ? a.ctl.n_in : a.views.totalRays;
+    if (items == 0) return cudaSuccess;
+    if (a.views.n < 1 || a.views.n > VT_MAX_VIEWS) return cudaErrorInvalidValue;
     unsigned int blocks;
-    if (a.ctl.susp_in == nullptr) {
-        int per = threads / (a.tile_w * a.tile_h);
-        if (per < 1 || threads % (a.tile_w * a.tile_h)) return cudaErrorInvalidValue;
-        long long tiles = (long long)((a.cam.W + a.tile_w - 1) / a.tile_w) * ((a.cam.H + a.tile_h - 1) / a.tile_h);
-        blocks = (unsigned int)((tiles + per - 1) / per);
+    if (persistent) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        unsigned int want = (items + threads - 1) / threads;
+        blocks = (unsigned int)(sms * (blocksPerSM > 0 ? blocksPerSM : 8));
+        if (blocks > want) blocks = want;
     } else {
-        if (a.ctl.n_in == 0) return cudaSuccess;
-        blocks = (a.ctl.n_in + threads - 1) / threads;
+        blocks = (items + threads - 1) / threads;
     }
-    if (blocks == 0) return cudaSuccess;
+#define VT_LAUNCH(V, S, P) k_trace<V, S, P><<<blocks, threads, 0, s>>>(a)
     if (a.br.vtype == 0) {
-        if (slabMode) k_trace<0, true><<<blocks, threads, 0, s>>>(a);
-        else k_trace<0, false><<<blocks, threads, 0, s>>>(a);
+        if (slabMode) { if (persistent) VT_LAUNCH(0, true, true); else VT_LAUNCH(0, true, false); }
+        else { if (persistent) VT_LAUNCH(0, false, true); else VT_LAUNCH(0, false, false); }
     } else {
-        if (slabMode) k_trace<1, true><<<blocks, threads, 0, s>>>(a);
-        else k_trace<1, false><<<blocks, threads, 0, s>>>(a);
+        if (slabMode) { if (persistent) VT_LAUNCH(1, true, true); else VT_LAUNCH(1, true, false); }
+        else { if (persistent) VT_LAUNCH(1, false, true); else VT_LAUNCH(1, false, false); }
     }
+#undef VT_LAUNCH
     return cudaGetLastError();
 }
 

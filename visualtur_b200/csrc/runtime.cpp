@@ -8,6 +8,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <stddef.h>
+
 #include <algorithm>
 #include <chrono>
 #include <vector>
@@ -138,10 +140,17 @@ extern "C" vt_status vt_render_cube(const vt_camera* c, const float* dev_cube, c
 /* ======================================================================== */
 /* Renderer handle                                                          */
 /* ======================================================================== */
+/* control block: one memset clears a pass's counters */
+struct CtlBlock {
+    unsigned long long counters[VT_C_COUNT];
+    unsigned int err;
+    unsigned int n_out, n_req, work;       /* reset every pass */
+    unsigned long long pool_used;
+};
+
 struct vt_handle {
     vt_params p;
     vt_options opt;
-    std::string volPath, dsName, octPath;
     vt_volume* vol = nullptr; bool ownVol = false;
     vt_octree* oct = nullptr; bool ownOct = false;
     vt_camera cam;
@@ -155,23 +164,23 @@ struct vt_handle {
     void* d_vol = nullptr; int P = 4; long long ve = 0;
     /* brick cache */
     vtrt::BrickCache* cache = nullptr;
-    /* per-ray buffers */
+    /* single-view output buffers */
     int nRays = 0;
     float4* d_rgba = nullptr; uint8_t* d_rgb8 = nullptr;
     unsigned long long* d_node = nullptr; unsigned long long* d_brick = nullptr; float* d_t = nullptr; float* d_n = nullptr;
     /* control */
-    unsigned long long* d_counters = nullptr;
-    unsigned int* d_err = nullptr;
-    unsigned int* d_nout = nullptr;       /* [0] n_out, [1] n_req */
-    unsigned long long* h_counters = nullptr;   /* pinned */
-    unsigned int* h_small = nullptr;             /* pinned: err, n_out, n_req */
-    /* suspended-ray ping-pong buffers */
-    unsigned int susp_cap = 0;
-    unsigned int* d_susp[2] = {nullptr, nullptr};
-    unsigned long long* d_stk[2] = {nullptr, nullptr};
-    unsigned char* d_top[2] = {nullptr, nullptr};
+    CtlBlock* d_ctl = nullptr; CtlBlock* h_ctl = nullptr;
+    DevView* d_views = nullptr; DevView* h_views = nullptr;
+    unsigned int* d_touched = nullptr; size_t touchedWords = 0;
+    /* suspended rays (ping-pong) */
+    unsigned int susp_cap = 0; unsigned long long pool_cap = 0;
+    SuspRec* d_susp[2] = {nullptr, nullptr};
+    unsigned long long* d_pool[2] = {nullptr, nullptr};
     unsigned long long* d_req = nullptr; unsigned int req_cap = 0;
-    std::vector<cudaEvent_t> ev;          /* start/stop pairs around trace launches */
+    /* timing and the pass-0 graph */
+    std::vector<cudaEvent_t> ev;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t s_int = nullptr;
     vt_stats stats;
     bool lastValid = false;
 };
@@ -179,11 +188,6 @@ struct vt_handle {
 static void free_ray_buffers(vt_handle* h) {
     cudaFree(h->d_rgba); cudaFree(h->d_rgb8); cudaFree(h->d_node); cudaFree(h->d_brick); cudaFree(h->d_t); cudaFree(h->d_n);
     h->d_rgba = nullptr; h->d_rgb8 = nullptr; h->d_node = nullptr; h->d_brick = nullptr; h->d_t = nullptr; h->d_n = nullptr;
-    for (int i = 0; i < 2; i++) {
-        cudaFree(h->d_susp[i]); cudaFree(h->d_stk[i]); cudaFree(h->d_top[i]);
-        h->d_susp[i] = nullptr; h->d_stk[i] = nullptr; h->d_top[i] = nullptr;
-    }
-    h->susp_cap = 0;
 }
 
 static vt_status alloc_ray_buffers(vt_handle* h) {
@@ -200,15 +204,20 @@ static vt_status alloc_ray_buffers(vt_handle* h) {
     return VT_OK;
 }
 
-static vt_status ensure_suspend_buffers(vt_handle* h, unsigned int cap) {
-    if (h->susp_cap >= cap) return VT_OK;
+/* suspended-ray records for `rays` rays and a stack pool of 12 entries per
+ * ray on average (rays whose stack does not fit restart from the root) */
+static vt_status ensure_suspend_buffers(vt_handle* h, unsigned int rays) {
+    if (h->susp_cap >= rays) return VT_OK;
     for (int i = 0; i < 2; i++) {
-        cudaFree(h->d_susp[i]); cudaFree(h->d_stk[i]); cudaFree(h->d_top[i]);
-        CK(cudaMalloc(&h->d_susp[i], (size_t)cap * 4));
-        CK(cudaMalloc(&h->d_stk[i], (size_t)cap * VT_STACK * 8));
-        CK(cudaMalloc(&h->d_top[i], (size_t)cap));
+        cudaFree(h->d_susp[i]); cudaFree(h->d_pool[i]);
+        h->d_susp[i] = nullptr; h->d_pool[i] = nullptr;
     }
-    h->susp_cap = cap;
+    h->susp_cap = rays;
+    h->pool_cap = (unsigned long long)rays * 12ull;
+    for (int i = 0; i < 2; i++) {
+        CK(cudaMalloc(&h->d_susp[i], (size_t)rays * sizeof(SuspRec)));
+        CK(cudaMalloc(&h->d_pool[i], (size_t)h->pool_cap * 8));
+    }
     return VT_OK;
 }
 
@@ -265,7 +274,7 @@ static vt_status upload_dense(vt_handle* h) {
     size_t bytes = (size_t)h->ve * h->ve * h->ve * es;
     CK(cudaMalloc(&h->d_vol, bytes));
     CK(cudaMemset(h->d_vol, 0, bytes));
-    /* stream the volume through a pinned staging buffer, x-slab by x-slab */
+    /* stream the volume through a mapped pinned staging buffer, x-slab by x-slab */
     const long long nx = v->dims[0], ny = v->dims[1], nz = v->dims[2];
     long long slab = std::max<long long>(1, (256ll << 20) / (ny * nz * (long long)es));
     void* stage = nullptr;
@@ -295,9 +304,14 @@ extern "C" void vt_default_options(vt_options* o) {
     o->record_trace = 0;
     o->trace_level = 4;
     o->record_hits = 1;
+    o->persistent = 0;
+    o->blocks_per_sm = 8;
+    o->pops = 8;
+    o->preload = 1;
+    o->use_graph = 1;
 }
 
-static vt_status validate(const vt_params* p, const vt_octree* o) {
+static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
     if (p->W <= 0 || p->H <= 0) return fail(VT_ERR_INVALID, "screen size must be positive");
     if (p->numRayPx != 1) return fail(VT_ERR_UNSUPPORTED, "numRayPx must be 1 (the reference generates W*H rays only)");
     if (p->octreeLevel < 1 || p->octreeLevel > o->nLevels) return fail(VT_ERR_INVALID, "octreeLevel %d outside 1..%d", p->octreeLevel, o->nLevels);
@@ -307,6 +321,12 @@ static vt_status validate(const vt_params* p, const vt_octree* o) {
     if (p->dimCubeCache[0] != b || p->dimCubeCache[1] != b || p->dimCubeCache[2] != b)
         return fail(VT_ERR_INVALID, "dimCubeCache must be %d^3 for levelCubes %d of a %d-level octree", b, p->levelCubes, o->nLevels);
     if (p->cubeInc < 3) return fail(VT_ERR_INVALID, "cubeInc must be >= 3 so every trilinear and normal tap stays in the brick");
+    if (opt) {
+        int tw = opt->tile_w, th = opt->tile_h;
+        if (tw <= 0 || th <= 0 || tw * th > 128 || 128 % (tw * th)) return fail(VT_ERR_INVALID, "tile %dx%d must divide 128 rays", tw, th);
+        if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
+            return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
+    }
     return VT_OK;
 }
 
@@ -319,11 +339,16 @@ static vt_status init_handle(vt_handle* h) {
     h->fovH = p.fov_H; h->fovW = p.fov_W;
     if ((s = vt_camera_init(&h->cam, p.H, p.W, p.distance, p.fov_H, p.fov_W)) != VT_OK) return s;
     if ((s = flatten_octree(h)) != VT_OK) return s;
-    CK(cudaMalloc(&h->d_counters, VT_C_COUNT * 8));
-    CK(cudaMalloc(&h->d_err, 4));
-    CK(cudaMalloc(&h->d_nout, 8));
-    CK(cudaHostAlloc(&h->h_counters, VT_C_COUNT * 8, cudaHostAllocDefault));
-    CK(cudaHostAlloc(&h->h_small, 16, cudaHostAllocDefault));
+    CK(cudaStreamCreateWithFlags(&h->s_int, cudaStreamNonBlocking));
+    CK(cudaMalloc(&h->d_ctl, sizeof(CtlBlock)));
+    CK(cudaHostAlloc(&h->h_ctl, sizeof(CtlBlock), cudaHostAllocDefault));
+    CK(cudaMalloc(&h->d_views, VT_MAX_VIEWS * sizeof(DevView)));
+    CK(cudaHostAlloc(&h->h_views, VT_MAX_VIEWS * sizeof(DevView), cudaHostAllocDefault));
+    if (h->opt.record_trace) {
+        h->touchedWords = std::max<size_t>(1, ((size_t)1 << (3 * h->opt.trace_level)) / 32);
+        CK(cudaMalloc(&h->d_touched, h->touchedWords * 4));
+        CK(cudaMemset(h->d_touched, 0, h->touchedWords * 4));
+    }
     if (h->opt.resident) {
         if ((s = upload_dense(h)) != VT_OK) return s;
     } else {
@@ -333,8 +358,7 @@ static vt_status init_handle(vt_handle* h) {
         cc.hostThreads = h->opt.host_threads;
         h->cache = new vtrt::BrickCache();
         if ((s = h->cache->init(cc)) != VT_OK) return s;
-        /* preload when every needed brick fits */
-        if ((size_t)p.maxElementsCache >= h->leafBricks.size()) {
+        if (h->opt.preload && (size_t)p.maxElementsCache >= h->leafBricks.size()) {
             if ((s = h->cache->preload(h->leafBricks)) != VT_OK) return s;
         }
         h->req_cap = (unsigned int)std::max<size_t>(h->leafBricks.size(), 1);
@@ -349,11 +373,13 @@ extern "C" vt_status vt_create_from(const vt_params* p, const vt_options* opt, v
                                     vt_handle** out) {
     clear_error();
     if (!p || !v || !o || !out) return fail(VT_ERR_INVALID, "vt_create_from: null argument");
-    vt_status s = validate(p, o);
+    vt_options dopt;
+    vt_default_options(&dopt);
+    vt_status s = validate(p, o, opt ? opt : &dopt);
     if (s != VT_OK) return s;
     vt_handle* h = new vt_handle();
     h->p = *p;
-    if (opt) h->opt = *opt; else vt_default_options(&h->opt);
+    h->opt = opt ? *opt : dopt;
     h->vol = v; h->oct = o;
     if ((s = init_handle(h)) != VT_OK) { vt_destroy(h); return s; }
     *out = h;
@@ -377,12 +403,17 @@ extern "C" vt_status vt_create(const vt_params* p, const vt_options* opt, vt_han
 
 extern "C" void vt_destroy(vt_handle* h) {
     if (!h) return;
+    if (h->s_int) cudaStreamSynchronize(h->s_int);
+    cudaDeviceSynchronize();
     free_ray_buffers(h);
     for (uint2* p : h->d_nodes) cudaFree(p);
-    cudaFree(h->d_vol); cudaFree(h->d_counters); cudaFree(h->d_err); cudaFree(h->d_nout); cudaFree(h->d_req);
-    if (h->h_counters) cudaFreeHost(h->h_counters);
-    if (h->h_small) cudaFreeHost(h->h_small);
+    for (int i = 0; i < 2; i++) { cudaFree(h->d_susp[i]); cudaFree(h->d_pool[i]); }
+    cudaFree(h->d_vol); cudaFree(h->d_ctl); cudaFree(h->d_views); cudaFree(h->d_req); cudaFree(h->d_touched);
+    if (h->h_ctl) cudaFreeHost(h->h_ctl);
+    if (h->h_views) cudaFreeHost(h->h_views);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->s_int) cudaStreamDestroy(h->s_int);
     delete h->cache;
     if (h->ownVol) vt_volume_close(h->vol);
     if (h->ownOct) vt_octree_free(h->oct);
@@ -430,6 +461,7 @@ extern "C" vt_status vt_change_cache(vt_handle* h, int nE, const int cDim[3], in
     if (cInc < 3) return fail(VT_ERR_INVALID, "cubeInc must be >= 3");
     if (h->opt.resident) { h->p.maxElementsCache = nE; return VT_OK; }
     vt_status s;
+    CK(cudaDeviceSynchronize());
     h->p.maxElementsCache = nE; h->p.cubeInc = cInc; h->inc = cInc; h->D = h->edge + 2 * cInc;
     delete h->cache;
     vtrt::CacheConfig cc;
@@ -437,15 +469,15 @@ extern "C" vt_status vt_change_cache(vt_handle* h, int nE, const int cDim[3], in
     cc.deviceSlots = nE; cc.hostSlots = h->p.maxElementsCache_CPU; cc.hostThreads = h->opt.host_threads;
     h->cache = new vtrt::BrickCache();
     if ((s = h->cache->init(cc)) != VT_OK) return s;
-    if ((size_t)nE >= h->leafBricks.size() && (s = h->cache->preload(h->leafBricks)) != VT_OK) return s;
+    if (h->opt.preload && (size_t)nE >= h->leafBricks.size() && (s = h->cache->preload(h->leafBricks)) != VT_OK) return s;
     h->lastValid = false;
     return VT_OK;
 }
 
 /* ---- frame ---------------------------------------------------------------- */
-static void fill_args(vt_handle* h, TraceArgs& a, float4* rgba, uint8_t* rgb8) {
+static void fill_args(vt_handle* h, TraceArgs& a, int nViews, unsigned int totalRays) {
     memset(&a, 0, sizeof(a));
-    a.cam = dev_camera(h->cam);
+    a.views.v = h->d_views; a.views.n = nViews; a.views.totalRays = totalRays;
     a.oct.nLevels = h->nLevels; a.oct.Lo = h->Lo; a.oct.Lc = h->Lc; a.oct.rootValid = h->rootValid;
     for (int l = 0; l < h->Lo; l++) a.oct.nodes[l] = h->d_nodes[l];
     a.br.vtype = h->vol->vtype; a.br.inc = h->inc;
@@ -455,89 +487,143 @@ static void fill_args(vt_handle* h, TraceArgs& a, float4* rgba, uint8_t* rgb8) {
     } else {
         h->cache->fill_args(a.br);
     }
-    a.out.rgba = rgba; a.out.rgb8 = rgb8;
-    a.out.node = h->d_node; a.out.brick = h->d_brick; a.out.t = h->d_t; a.out.n = h->d_n;
-    a.ctl.counters = h->d_counters; a.ctl.err = h->d_err;
-    a.ctl.n_out = h->d_nout; a.ctl.n_req = h->d_nout + 1;
+    if (nViews == 1) { a.out.node = h->d_node; a.out.brick = h->d_brick; a.out.t = h->d_t; a.out.n = h->d_n; }
+    CtlBlock* c = h->d_ctl;
+    a.ctl.counters = c->counters; a.ctl.err = &c->err; a.ctl.work = &c->work;
+    a.ctl.n_out = &c->n_out; a.ctl.n_req = &c->n_req; a.ctl.pool_used = &c->pool_used;
     a.ctl.req = h->d_req; a.ctl.req_cap = h->req_cap;
     a.ctl.lookahead = h->opt.lookahead;
+    if (h->d_touched) {
+        a.ctl.touched = h->d_touched;
+        a.ctl.touch_shift = 3 * (h->Lo - h->opt.trace_level);
+        a.ctl.touch_base = 1ull << (3 * h->opt.trace_level);
+    }
     a.iso = h->oct->iso;
     a.light = make_float3(0.0f, 512.0f, 0.0f);   /* src/visualTur.cu:30 */
     a.tile_w = h->opt.tile_w; a.tile_h = h->opt.tile_h;
+    a.pops = h->opt.pops > 0 ? h->opt.pops : 8;
 }
 
 static vt_status collect_counters(vt_handle* h, cudaStream_t s) {
-    CK(cudaMemcpyAsync(h->h_counters, h->d_counters, VT_C_COUNT * 8, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(h->h_small, h->d_err, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CtlBlock), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    const unsigned long long* c = h->h_counters;
+    const unsigned long long* c = h->h_ctl->counters;
     vt_stats& st = h->stats;
     st.rays += c[VT_C_RAYS]; st.hits += c[VT_C_HITS]; st.samples += c[VT_C_SAMPLES];
     st.normal_samples += c[VT_C_NSAMPLES]; st.candidates += c[VT_C_CANDIDATES]; st.expansions += c[VT_C_EXPANSIONS];
     st.device_hits += c[VT_C_DEVHITS]; st.device_misses += c[VT_C_DEVMISSES];
     st.max_stack = std::max<int64_t>(st.max_stack, (int64_t)c[VT_C_MAXSTACK]);
-    unsigned int err = h->h_small[0];
+    unsigned int err = h->h_ctl->err;
     if (err & VT_KERR_STACK) return fail(VT_ERR_STACK, "a ray's traversal stack overflowed (%d entries)", VT_STACK);
     if (err & VT_KERR_NOTRESIDENT) return fail(VT_ERR_STATE, "resident render met a brick with no slot");
     if (err & (VT_KERR_SUSPEND_FULL | VT_KERR_REQUEST_FULL)) return fail(VT_ERR_STATE, "demand-paging queue overflow (%u)", err);
     return VT_OK;
 }
 
-/* records the launch of pass `k` between events 2k and 2k+1 */
-static vt_status timed_trace(vt_handle* h, const TraceArgs& a, bool slabMode, cudaStream_t s, int k) {
+/* trace launch of pass `k`, between events 2k and 2k+1 */
+static vt_status ensure_events(vt_handle* h, int k) {
     while ((int)h->ev.size() < 2 * (k + 1)) {
         cudaEvent_t e;
         CK(cudaEventCreate(&e));
         h->ev.push_back(e);
     }
-    CK(cudaEventRecord(h->ev[2 * k], s));
-    CK(vt_launch_trace(a, slabMode, s));
-    CK(cudaEventRecord(h->ev[2 * k + 1], s));
-    h->stats.launches++;
     return VT_OK;
 }
 
-static vt_status render_frame(vt_handle* h, float4* rgba, uint8_t* rgb8, cudaStream_t s) {
+/* pass 0: clear the control block (and trace log), upload the view table,
+ * launch the trace kernel -- captured once as a CUDA graph and replayed */
+static vt_status pass0(vt_handle* h, const TraceArgs& a, int nViews, bool slabMode, cudaStream_t s) {
+    auto enqueue = [&](cudaStream_t q) -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(h->d_ctl, 0, sizeof(CtlBlock), q);
+        if (e == cudaSuccess && h->d_touched) e = cudaMemsetAsync(h->d_touched, 0, h->touchedWords * 4, q);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_views, h->h_views, (size_t)nViews * sizeof(DevView), cudaMemcpyHostToDevice, q);
+        if (e == cudaSuccess) e = vt_launch_trace(a, slabMode, h->opt.persistent != 0, h->opt.blocks_per_sm, q);
+        return e;
+    };
+    if (!h->opt.use_graph || s == 0) {
+        CK(enqueue(s));
+        return VT_OK;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue(s);
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(VT_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    bool ok = false;
+    if (h->graph) {
+        cudaGraphExecUpdateResultInfo info;
+        ok = cudaGraphExecUpdate(h->graph, g, &info) == cudaSuccess;
+        if (!ok) { cudaGetLastError(); cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    }
+    if (!ok) {
+        e = cudaGraphInstantiate(&h->graph, g, 0);
+        if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(VT_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    }
+    cudaGraphDestroy(g);
+    CK(cudaGraphLaunch(h->graph, s));
+    return VT_OK;
+}
+
+struct ViewReq { vt_camera cam; float4* rgba; uint8_t* rgb8; };
+
+static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream_t s) {
     auto t0 = std::chrono::steady_clock::now();
+    if (n < 1 || n > VT_MAX_VIEWS) return fail(VT_ERR_INVALID, "1..%d views per call", VT_MAX_VIEWS);
+    const int tw = h->opt.tile_w, th = h->opt.tile_h;
+    unsigned long long base = 0, real = 0;
+    for (int k = 0; k < n; k++) {
+        const vt_camera& c = vr[k].cam;
+        if (c.W <= 0 || c.H <= 0) return fail(VT_ERR_INVALID, "view %d has no pixels", k);
+        DevView& v = h->h_views[k];
+        v.cam = dev_camera(c);
+        v.rgba = vr[k].rgba; v.rgb8 = vr[k].rgb8;
+        v.rayBase = (unsigned int)base;
+        v.tilesX = (unsigned int)((c.W + tw - 1) / tw);
+        base += (unsigned long long)v.tilesX * ((c.H + th - 1) / th) * (unsigned long long)(tw * th);
+        real += (unsigned long long)c.W * c.H;
+    }
+    if (base > 0xFFFFFFFFull) return fail(VT_ERR_UNSUPPORTED, "more than 2^32 rays in one call");
     TraceArgs a;
-    fill_args(h, a, rgba, rgb8);
-    CK(cudaMemsetAsync(h->d_counters, 0, VT_C_COUNT * 8, s));
-    CK(cudaMemsetAsync(h->d_err, 0, 4, s));
-    CK(cudaMemsetAsync(h->d_nout, 0, 8, s));
+    fill_args(h, a, n, (unsigned int)base);
     const bool slabMode = !h->opt.resident;
     const bool allResident = h->opt.resident || h->cache->all_resident();
-    if (!allResident) {
-        vt_status st = ensure_suspend_buffers(h, (unsigned int)h->nRays);
-        if (st != VT_OK) return st;
-    }
-    if (slabMode) h->cache->begin_frame();
-    a.ctl.susp_cap = h->susp_cap;
-    a.ctl.susp_out = h->d_susp[0]; a.ctl.stk_out = h->d_stk[0]; a.ctl.top_out = h->d_top[0];
-    if (slabMode) a.br.pass = h->cache->next_pass();
-    vt_status st0 = timed_trace(h, a, slabMode, s, 0);
-    if (st0 != VT_OK) return st0;
+    vt_status st;
+    if (!allResident && (st = ensure_suspend_buffers(h, (unsigned int)real)) != VT_OK) return st;
+    a.ctl.out_cap = h->susp_cap; a.ctl.pool_cap = h->pool_cap;
+    a.ctl.out = h->d_susp[0]; a.ctl.pool_out = h->d_pool[0];
+    if (slabMode) { h->cache->begin_frame(); a.br.pass = h->cache->next_pass(); }
+    if ((st = ensure_events(h, 0)) != VT_OK) return st;
+    CK(cudaEventRecord(h->ev[0], s));
+    if ((st = pass0(h, a, n, slabMode, s)) != VT_OK) return st;
+    CK(cudaEventRecord(h->ev[1], s));
+    h->stats.launches++;
     int passes = 1;
     double stall = 0, h2d = 0;
-    vt_status st;
     if (!allResident) {
         int cur = 0;
         for (;;) {
-            CK(cudaMemcpyAsync(h->h_small, h->d_nout, 8, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(&h->h_ctl->n_out, &h->d_ctl->n_out, 8, cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
-            unsigned int nOut = h->h_small[0], nReq = h->h_small[1];
+            unsigned int nOut = h->h_ctl->n_out, nReq = h->h_ctl->n_req;
             if (nOut == 0) break;
+            if (nOut > h->susp_cap) return fail(VT_ERR_STATE, "suspended-ray list overflow");
             if (passes >= h->opt.max_passes) return fail(VT_ERR_TIMEOUT, "frame did not finish in %d passes", passes);
             auto ts = std::chrono::steady_clock::now();
             if ((st = h->cache->service(h->d_req, nReq, s, &h2d)) != VT_OK) return st;
             stall += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();
-            /* resume the suspended rays */
-            a.ctl.susp_in = h->d_susp[cur]; a.ctl.n_in = nOut;
-            a.ctl.stk_in = h->d_stk[cur]; a.ctl.top_in = h->d_top[cur];
+            a.ctl.in = h->d_susp[cur]; a.ctl.n_in = nOut; a.ctl.pool_in = h->d_pool[cur];
             cur ^= 1;
-            a.ctl.susp_out = h->d_susp[cur]; a.ctl.stk_out = h->d_stk[cur]; a.ctl.top_out = h->d_top[cur];
+            a.ctl.out = h->d_susp[cur]; a.ctl.pool_out = h->d_pool[cur];
             a.br.pass = h->cache->next_pass();
-            CK(cudaMemsetAsync(h->d_nout, 0, 8, s));
-            if ((st = timed_trace(h, a, slabMode, s, passes)) != VT_OK) return st;
+            CK(cudaMemsetAsync(&h->d_ctl->n_out, 0, offsetof(CtlBlock, pool_used) + 8 - offsetof(CtlBlock, n_out), s));
+            if ((st = ensure_events(h, passes)) != VT_OK) return st;
+            CK(cudaEventRecord(h->ev[2 * passes], s));
+            CK(vt_launch_trace(a, slabMode, h->opt.persistent != 0, h->opt.blocks_per_sm, s));
+            CK(cudaEventRecord(h->ev[2 * passes + 1], s));
+            h->stats.launches++;
             passes++;
         }
     }
@@ -555,39 +641,91 @@ static vt_status render_frame(vt_handle* h, float4* rgba, uint8_t* rgb8, cudaStr
     h->stats.bytes_h2d_last_frame = h2d;
     if (h->cache) h->cache->fold_stats(h->stats);
     h->stats.ms_last_frame = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    h->lastValid = true;
+    h->lastValid = n == 1;
     return VT_OK;
 }
 
 extern "C" vt_status vt_render(vt_handle* h, float* dev_rgba, uint8_t* dev_rgb8, void* stream) {
     clear_error();
     if (!h) return fail(VT_ERR_INVALID, "null handle");
-    if (!dev_rgba && !dev_rgb8) { dev_rgba = (float*)h->d_rgba; }
-    return render_frame(h, (float4*)dev_rgba, dev_rgb8, (cudaStream_t)stream);
+    ViewReq v = {h->cam, dev_rgba ? (float4*)dev_rgba : (dev_rgb8 ? nullptr : h->d_rgba), dev_rgb8};
+    return render_views(h, &v, 1, (cudaStream_t)stream);
 }
 
 extern "C" vt_status vt_render_host(vt_handle* h, float* host_rgba, uint8_t* host_rgb8) {
     clear_error();
     if (!h) return fail(VT_ERR_INVALID, "null handle");
-    vt_status s = render_frame(h, h->d_rgba, host_rgb8 ? h->d_rgb8 : nullptr, 0);
+    ViewReq v = {h->cam, host_rgba ? h->d_rgba : nullptr, host_rgb8 ? h->d_rgb8 : nullptr};
+    if (!v.rgba && !v.rgb8) v.rgba = h->d_rgba;
+    vt_status s = render_views(h, &v, 1, h->s_int);
     if (s != VT_OK) return s;
     size_t n = (size_t)h->nRays;
-    if (host_rgba) CK(cudaMemcpy(host_rgba, h->d_rgba, n * 16, cudaMemcpyDeviceToHost));
-    if (host_rgb8) CK(cudaMemcpy(host_rgb8, h->d_rgb8, n * 3, cudaMemcpyDeviceToHost));
+    if (host_rgba) CK(cudaMemcpyAsync(host_rgba, h->d_rgba, n * 16, cudaMemcpyDeviceToHost, h->s_int));
+    if (host_rgb8) CK(cudaMemcpyAsync(host_rgb8, h->d_rgb8, n * 3, cudaMemcpyDeviceToHost, h->s_int));
+    CK(cudaStreamSynchronize(h->s_int));
     return VT_OK;
+}
+
+extern "C" vt_status vt_render_batch(vt_handle* h, const vt_view* views, int n, void* stream) {
+    clear_error();
+    if (!h || !views || n < 1) return fail(VT_ERR_INVALID, "vt_render_batch: bad arguments");
+    std::vector<ViewReq> vr(n);
+    for (int k = 0; k < n; k++) {
+        if (!views[k].dev_rgba && !views[k].dev_rgb8) return fail(VT_ERR_INVALID, "view %d has no output buffer", k);
+        vr[k].cam = views[k].cam; vr[k].rgba = (float4*)views[k].dev_rgba; vr[k].rgb8 = views[k].dev_rgb8;
+    }
+    return render_views(h, vr.data(), n, (cudaStream_t)stream);
 }
 
 extern "C" vt_status vt_debug_hits(vt_handle* h, uint64_t* node, uint64_t* brick, float* t, float* n) {
     clear_error();
     if (!h) return fail(VT_ERR_INVALID, "null handle");
     if (!h->opt.record_hits) return fail(VT_ERR_STATE, "record_hits is off");
-    if (!h->lastValid) return fail(VT_ERR_STATE, "no frame rendered since the last change");
+    if (!h->lastValid) return fail(VT_ERR_STATE, "no single-view frame rendered since the last change");
     size_t N = (size_t)h->nRays;
     CK(cudaDeviceSynchronize());
     if (node) CK(cudaMemcpy(node, h->d_node, N * 8, cudaMemcpyDeviceToHost));
     if (brick) CK(cudaMemcpy(brick, h->d_brick, N * 8, cudaMemcpyDeviceToHost));
     if (t) CK(cudaMemcpy(t, h->d_t, N * 4, cudaMemcpyDeviceToHost));
     if (n) CK(cudaMemcpy(n, h->d_n, N * 12, cudaMemcpyDeviceToHost));
+    return VT_OK;
+}
+
+extern "C" vt_status vt_get_trace(vt_handle* h, uint32_t* bits, int64_t nwords) {
+    clear_error();
+    if (!h || !bits) return fail(VT_ERR_INVALID, "null argument");
+    if (!h->d_touched) return fail(VT_ERR_STATE, "record_trace is off");
+    if ((size_t)nwords < h->touchedWords) return fail(VT_ERR_INVALID, "need %zu words", h->touchedWords);
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(bits, h->d_touched, h->touchedWords * 4, cudaMemcpyDeviceToHost));
+    return VT_OK;
+}
+
+extern "C" vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n, int64_t* loaded, void* stream) {
+    clear_error();
+    if (!h || (!bricks && n > 0)) return fail(VT_ERR_INVALID, "null argument");
+    if (loaded) *loaded = 0;
+    if (h->opt.resident || n <= 0) return VT_OK;
+    uint64_t lo = 1ull << (3 * h->Lc), hi = lo << 3;
+    std::vector<uint64_t> b;
+    b.reserve((size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+        if (bricks[i] < lo || bricks[i] >= hi) return fail(VT_ERR_INVALID, "brick code %llu not at levelCubes", (unsigned long long)bricks[i]);
+        b.push_back(bricks[i]);
+    }
+    int64_t got = 0;
+    vt_status s = h->cache->prefetch(b, stream ? (cudaStream_t)stream : h->s_int, &got);
+    if (loaded) *loaded = got;
+    h->cache->fold_stats(h->stats);
+    return s;
+}
+
+extern "C" vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n) {
+    clear_error();
+    if (!h || !n) return fail(VT_ERR_INVALID, "null argument");
+    int64_t cap = *n;
+    *n = (int64_t)h->leafBricks.size();
+    if (bricks) memcpy(bricks, h->leafBricks.data(), (size_t)std::min<int64_t>(cap, *n) * 8);
     return VT_OK;
 }
 
@@ -603,10 +741,4 @@ extern "C" vt_status vt_reset_stats(vt_handle* h) {
     memset(&h->stats, 0, sizeof(h->stats));
     if (h->cache) h->cache->reset_stats();
     return VT_OK;
-}
-
-extern "C" vt_status vt_render_batch(vt_handle* h, const vt_view* views, int n, void* stream) {
-    clear_error();
-    if (!h || (!views && n > 0)) return fail(VT_ERR_INVALID, "null argument");
-    return fail(VT_ERR_UNSUPPORTED, "vt_render_batch is not built yet");
 }

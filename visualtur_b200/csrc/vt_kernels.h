@@ -46,31 +46,55 @@ struct DevBricks {
     unsigned int pass;
 };
 
+/* Per-ray diagnostics, pixel-indexed for view 0 (single-view renders). */
 struct DevOut {
-    float4* rgba;
-    uint8_t* rgb8;
     unsigned long long* node;
     unsigned long long* brick;
     float* t;
     float* n;
 };
 
-/* Per-frame control: counters, error bits, demand paging queues. */
+/* One camera view of a batch.  Rays are numbered in tile order: view v owns
+ * the padded ray indices [rayBase, rayBase + tilesX*tilesY*tw*th). */
+#define VT_MAX_VIEWS 64
+struct DevView {
+    DevCamera cam;
+    float4* rgba;
+    uint8_t* rgb8;
+    unsigned int rayBase;
+    unsigned int tilesX;
+};
+struct DevViews {
+    const DevView* v;
+    int n;
+    unsigned int totalRays;
+};
+
+/* A suspended ray: padded global ray index, saved stack depth (0 = restart
+ * from the root) and offset of its entries in the stack pool. */
+struct SuspRec {
+    unsigned int ray;
+    unsigned int depth;
+    unsigned long long off;
+};
+
+/* Per-pass control: counters, error bits, work queue, demand paging. */
 struct DevCtl {
     unsigned long long* counters;
     unsigned int* err;
-    /* suspended rays: ray ids and saved stacks (in: this pass, out: next) */
-    const unsigned int* susp_in; unsigned int n_in;   /* rays to resume (NULL: all) */
-    const unsigned long long* stk_in; const unsigned char* top_in;
-    unsigned int* susp_out; unsigned int* n_out; unsigned int susp_cap;
-    unsigned long long* stk_out; unsigned char* top_out;
-    /* brick requests */
+    unsigned int* work;                         /* persistent-kernel work counter */
+    const SuspRec* in; unsigned int n_in;      /* rays to resume (NULL: pass 0) */
+    const unsigned long long* pool_in;
+    SuspRec* out; unsigned int* n_out; unsigned int out_cap;
+    unsigned long long* pool_out; unsigned long long* pool_used; unsigned long long pool_cap;
     unsigned long long* req; unsigned int* n_req; unsigned int req_cap;
-    int lookahead;
+    int lookahead;                              /* bricks a suspended ray may request ahead */
+    unsigned int* touched; int touch_shift;     /* optional bitmask of coarse nodes used (trace log) */
+    unsigned long long touch_base;
 };
 
 struct TraceArgs {
-    DevCamera cam;
+    DevViews views;
     DevOctree oct;
     DevBricks br;
     DevOut out;
@@ -78,10 +102,11 @@ struct TraceArgs {
     float iso;
     float3 light;
     int tile_w, tile_h;
+    int pops;                                   /* pops between warp refills (persistent) */
 };
 
 /* launchers (render.cu) */
-cudaError_t vt_launch_trace(const TraceArgs& a, bool slab, cudaStream_t s);
+cudaError_t vt_launch_trace(const TraceArgs& a, bool slab, bool persistent, int blocks_per_sm, cudaStream_t s);
 cudaError_t vt_launch_rays(const DevCamera& c, float* dirs, cudaStream_t s);
 cudaError_t vt_launch_cube(const DevCamera& c, const float* cube, int3 minBox, int3 cubeDim,
                            int3 cubeInc, float iso, float3 light, float4* rgba, cudaStream_t s);
