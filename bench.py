@@ -56,11 +56,13 @@ CONFIGS = {
 }
 
 # renderer modes: "plain" = the reference's scheme (one view per launch,
-# demand LRU from a cold cache); "best" = persistent ray queue + lookahead
-# requests (the product's default for the fly-through)
+# demand LRU from a cold cache, no prefetch); "best" = the product: batches
+# of 8 frames per persistent ray-queue launch, lookahead requests, learned
+# prefetch hints for the next batch, kernel knobs from the autotuner
 MODES = {
-    "plain": dict(persistent=0, lookahead=0, use_graph=0),
-    "best": dict(persistent=1, lookahead=2, use_graph=1, pops=8, blocks_per_sm=8),
+    "plain": dict(opts=dict(persistent=0, lookahead=0, use_graph=0), batch=1, learned=False, autotune=False),
+    "best": dict(opts=dict(persistent=1, lookahead=2, use_graph=1, pops=8, blocks_per_sm=8), batch=8,
+                 learned=True, autotune=True),
 }
 
 
@@ -183,8 +185,37 @@ class Workload:
     def renderer(self, mode):
         """A renderer in `mode` (cold cache unless the workload is resident)."""
         opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=0,
-                                      preload=1 if self.cfg["resident"] else 0, **MODES[mode])
+                                      preload=1 if self.cfg["resident"] else 0, **MODES[mode]["opts"])
         return self.vt.visualTur(self.params, opt, volume=self.fm, octree=self.oc)
+
+    def train_prefetcher(self, torch, poses=20000, paths=100, W=240, H=135, epochs=30):
+        """Learned prefetch: traces from random fly-throughs (radius
+        2500-3500 scaled to the volume) rendered at W x H by a resident
+        renderer with the access log, then GPU training of the network."""
+        from visualtur_b200 import prefetch as pf
+        vt, cfg, n = self.vt, self.cfg, self.cfg["n"]
+        t0 = time.time()
+        p = vt.make_params(W=W, H=H, octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"],
+                           levelCubes=cfg["levelC"], dimCube=1 << (self.oc.nLevels - cfg["levelC"]),
+                           cubeInc=cfg["inc"], distance=cfg["dist"], fov_H=cfg["fov"], fov_W=cfg["fov"])
+        tr = vt.visualTur(p, vt.default_options(resident=1, record_trace=1, trace_level=pf.TRACE_LEVEL,
+                                                record_hits=0), volume=self.fm, octree=self.oc)
+        scale = n / 2048.0
+        X, Y = pf.collect_traces(tr, n, W, H, cfg["fov"], np.random.default_rng(7), paths, poses // paths,
+                                 2500 * scale, 3500 * scale, dist=cfg["dist"])
+        bricks = tr.brick_list()
+        tr.close()
+        torch.cuda.empty_cache()
+        t1 = time.time()
+        P = pf.Prefetcher(n, cfg["fov"], cfg["levelC"], bricks, seed=11)
+        hist = P.train(torch, X, Y, epochs=epochs, batch=256, lr=1e-3)
+        t2 = time.time()
+        self.train_info = {"poses": int(X.shape[0]), "trace_res": [W, H], "positive_frac": round(float(Y.mean()), 4),
+                           "epochs": epochs, "loss_first": round(hist[0], 4), "loss_last": round(hist[-1], 4),
+                           "trace_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1)}
+        log("prefetch: %d traces in %.1fs, training %.1fs, loss %.4f -> %.4f" %
+            (X.shape[0], t1 - t0, t2 - t1, hist[0], hist[-1]))
+        return P
 
 
 def roofline(stats_frames, trace_ms, pixels):
@@ -241,40 +272,84 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, frame=0):
 
 
 # ----------------------------------------------------------------------------- arms
-def timed_frames(wl, r, cfg, torch, dev, stream, frame0, warmup, steps, dist, clocks=None):
-    """Renders warmup + steps consecutive frames; returns per-frame device ms
-    (CUDA events on the launching stream) and per-frame stats."""
-    W, H = cfg["W"], cfg["H"]
-    sp = stream.cuda_stream
-    rgba = torch.empty(W * H * 4, dtype=torch.float32, device=dev)
-    rgb8 = torch.empty(W * H * 3, dtype=torch.uint8, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if cfg["l2flush"] else None
+class Launcher:
+    """Renders consecutive orbit frames in launches of `batch` views; with a
+    predictor, hands the renderer the predicted bricks of the next launch."""
+
+    def __init__(self, wl, r, cfg, torch, dev, stream, batch=1, predictor=None, threshold=0.25):
+        self.wl, self.r, self.cfg, self.torch, self.stream = wl, r, cfg, torch, stream
+        self.batch, self.P, self.thr = batch, predictor, threshold
+        W, H = cfg["W"], cfg["H"]
+        self.bufs = [(torch.empty(W * H * 4, dtype=torch.float32, device=dev),
+                      torch.empty(W * H * 3, dtype=torch.uint8, device=dev)) for _ in range(batch)]
+
+    def cams(self, f0, n):
+        return [frame_camera(self.wl.vt, self.cfg, f0 + i) for i in range(n)]
+
+    def hint(self, cams):
+        if self.P is None or not cams:
+            return
+        from visualtur_b200 import prefetch as pf
+        feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for c in cams])
+        probs = self.P.predict(self.torch, feats).max(axis=0)
+        self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
+
+    def launch(self, cams, next_cams=()):
+        self.hint(list(next_cams))
+        sp = self.stream.cuda_stream
+        if self.batch == 1:
+            self.r.set_camera(cams[0])
+            self.r.updateVisibleCubes(self.bufs[0][0], self.bufs[0][1], stream=sp)
+            return
+        views = []
+        for c, (a, b) in zip(cams, self.bufs):
+            v = self.wl.vt.vt_view()
+            v.cam, v.dev_rgba, v.dev_rgb8 = c, a.data_ptr(), b.data_ptr()
+            views.append(v)
+        self.r.render_batch(views, stream=sp)
+
+
+def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
+    """Renders `warmup` then `steps` consecutive frames in launches of
+    L.batch; returns device ms (CUDA events on the launching stream) and
+    stats per launch, and the number of frames in each."""
+    torch, r, stream = L.torch, L.r, L.stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=L.bufs[0][0].device) if flush_l2 else None
     with torch.cuda.stream(stream):
-        for i in range(warmup):
-            r.set_camera(frame_camera(wl.vt, cfg, frame0 + i))
-            r.updateVisibleCubes(rgba, rgb8, stream=sp)
+        f = frame0
+        while f < frame0 + warmup:
+            n = min(L.batch, frame0 + warmup - f)
+            nxt = min(L.batch, frame0 + warmup + steps - f - n)
+            L.launch(L.cams(f, n), L.cams(f + n, nxt))
+            f += n
         torch.cuda.synchronize()
         r.reset_stats()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        per_frame = []
+        launches = []
+        f = frame0 + warmup
+        while f < frame0 + warmup + steps:
+            n = min(L.batch, frame0 + warmup + steps - f)
+            nxt = min(L.batch, frame0 + warmup + steps - f - n)
+            launches.append((f, n, L.cams(f, n), L.cams(f + n, nxt)))
+            f += n
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in launches]
+        per = []
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         if clocks:
             clocks.start()
-        for i in range(steps):
+        for k, (f0, n, cams, nxt) in enumerate(launches):
             if flush is not None:
                 flush.zero_()
-            r.set_camera(frame_camera(wl.vt, cfg, frame0 + warmup + i))
-            ev[i][0].record(stream)
-            r.updateVisibleCubes(rgba, rgb8, stream=sp)
-            ev[i][1].record(stream)
-            per_frame.append(r.stats())
+            ev[k][0].record(stream)
+            L.launch(cams, nxt)
+            ev[k][1].record(stream)
+            per.append(r.stats())
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
     clk = clocks.stop() if clocks else None
-    return [a.elapsed_time(b) for a, b in ev], per_frame, clk
+    return [a.elapsed_time(b) for a, b in ev], per, [n for _, n, _, _ in launches], clk
 
 
 def frame_deltas(per_frame):
@@ -289,16 +364,29 @@ def run_ours(args, cfg, rank, world, torch, dist):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     work = tempfile.mkdtemp(prefix="vtbench_")
+    M = MODES[args.mode]
     wl = Workload(cfg, torch, dev, work, mode=args.mode)
     W, H = cfg["W"], cfg["H"]
     stream = torch.cuda.Stream(device=dev)
     frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
-    ms, per_frame, clk = timed_frames(wl, wl.r, cfg, torch, dev, stream, frame0, args.warmup, args.steps, dist,
-                                      Clocks(dev.index))
+    batch = 1 if cfg["resident"] else M["batch"]
+    P = wl.train_prefetcher(torch) if (M["learned"] and not cfg["resident"] and not args.no_learned) else None
+    tune = None
+    if M["autotune"] and not args.no_autotune:
+        from visualtur_b200 import autotune as at
+        Ltune = Launcher(wl, wl.r, cfg, torch, dev, stream, batch=batch)
+        cams = Ltune.cams(frame0, batch)
+        best, table = at.tune_schedule(torch, wl.r, lambda rr, i, s_: Ltune.launch(cams), frames=3, stream=stream)
+        tune = {"best": best, "points": len(table), "table": table}
+        log("autotune: best %s" % best)
+        if not cfg["resident"]:
+            wl.r.drop_cache()     # the timed run starts from a cold cache
+    L = Launcher(wl, wl.r, cfg, torch, dev, stream, batch=batch, predictor=P)
+    ms, per, nfr, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index), cfg["l2flush"])
     tot_ms = sum(ms)
     st = wl.r.stats()
-    fd = frame_deltas(per_frame)
-    trace_tot = sum(s["ms_trace_last_frame"] for s in per_frame)
+    ld = frame_deltas(per)
+    trace_tot = sum(s["ms_trace_last_frame"] for s in per)
     rays_rank = W * H * args.steps
     t_max = tot_ms
     if dist:
@@ -306,30 +394,40 @@ def run_ours(args, cfg, rank, world, torch, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = rays_rank * world / (t_max * 1e-3)
-    # end to end: public API with host output buffers (pose in, RGB8 image out)
-    import ctypes
-    e2e_steps = max(2, min(args.steps, 30))
-    out8 = np.empty((W * H, 3), np.uint8)
+    # end to end through the public API: poses in, RGB8 images back in pinned host memory
+    e2e_frames = max(batch, 2 * batch if batch > 1 else 30)
+    host8 = [torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True) for _ in range(batch)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for i in range(e2e_steps):
-        wl.r.set_camera(frame_camera(wl.vt, cfg, frame0 + args.warmup + args.steps + i))
-        wl.vt.check(wl.vt.lib().vt_render_host(wl.r._h, None, out8.ctypes.data))
+    f = frame0 + args.warmup + args.steps
+    with torch.cuda.stream(stream):
+        for k in range(0, e2e_frames, batch):
+            cams = L.cams(f + k, batch)
+            L.launch(cams, L.cams(f + k + batch, batch))
+            for b in range(batch):
+                host8[b].copy_(L.bufs[b][1], non_blocking=True)
+            stream.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e = {"value": round(W * H * e2e_steps / e2e_s * world, 1), "unit": "rays/s",
+    import ctypes
+    e2e = {"value": round(W * H * e2e_frames / e2e_s * world, 1), "unit": "rays/s",
            "h2d_bytes_per_step": ctypes.sizeof(wl.vt.vt_camera), "d2h_bytes_per_step": W * H * 3,
-           "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3), "steps": e2e_steps,
-           "note": "continues the fly-through after the timed frames; wall clock around the synchronous host API"}
+           "ms_per_step": round(e2e_s * 1e3 / e2e_frames, 3), "steps": e2e_frames,
+           "note": "continues the fly-through after the timed frames; wall clock around the public API "
+                   "(vt_render / vt_render_batch) plus the D2H copy of every RGB8 frame"}
     # the plain LRU renderer on the same frames, for comparison
     plain = None
     if args.mode != "plain" and not cfg["resident"] and not args.no_plain:
         wl.r.close()
         rp = wl.renderer("plain")
-        pms, pper, _ = timed_frames(wl, rp, cfg, torch, dev, stream, frame0, args.warmup, args.steps, dist)
+        Lp = Launcher(wl, rp, cfg, torch, dev, stream, batch=1)
+        pms, pper, _, _ = timed_frames(Lp, frame0, args.warmup, args.steps, dist)
+        ps = rp.stats()
         plain = {"value": round(rays_rank * world / (sum(pms) * 1e-3), 1), "unit": "rays/s",
                  "ms_per_step": round(sum(pms) / args.steps, 4),
                  "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in pper) / args.steps, 4),
-                 "passes_per_step": round(sum(s["passes"] for s in pper) / args.steps, 3)}
+                 "passes_per_step": round(sum(s["passes"] for s in pper) / args.steps, 3),
+                 "device_hit_rate": round(ps["device_hits"] / max(1, ps["device_hits"] + ps["device_misses"]), 5),
+                 "bricks_loaded": ps["bricks_loaded_disk"]}
         rp.close()
     if rank != 0:
         return None
@@ -340,22 +438,29 @@ def run_ours(args, cfg, rank, world, torch, dist):
         "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, device-generated)",
         "config": {"workload": cfg["workload"], "name": args.config, "mode": args.mode, "W": W, "H": H,
+                   "frames_per_launch": batch, "learned_prefetch": P is not None,
                    "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": roofline(fd, trace_tot, W * H * args.steps),
+        "roofline": roofline(ld, trace_tot, W * H * args.steps),
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": int(st["launches"]),
-        "frame_stats": {"passes_per_step": round(sum(s["passes"] for s in per_frame) / args.steps, 3),
-                        "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in per_frame) / args.steps, 4),
+        "frame_stats": {"passes_per_launch": round(sum(s["passes"] for s in per) / len(per), 3),
+                        "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in per) / args.steps, 4),
+                        "prefetch_ms_per_step": round(sum(s["ms_prefetch_last_frame"] for s in per) / args.steps, 4),
                         "trace_ms_per_step": round(trace_tot / args.steps, 4),
-                        "bricks_requested": st["bricks_requested"], "bricks_loaded_disk": st["bricks_loaded_disk"],
-                        "device_hits": st["device_hits"], "device_misses": st["device_misses"],
+                        "device_hit_rate": round(st["device_hits"] / max(1, st["device_hits"] + st["device_misses"]), 5),
+                        "bricks_requested": st["bricks_requested"], "bricks_loaded": st["bricks_loaded_disk"],
+                        "bricks_prefetched": st["bricks_prefetched"],
                         "hits": st["hits"], "samples": st["samples"], "candidates": st["candidates"],
                         "expansions": st["expansions"]},
     }
     if plain:
         line["plain_lru"] = plain
+    if P is not None:
+        line["learned_prefetch"] = wl.train_info
+    if tune:
+        line["autotune"] = {"best": tune["best"], "points": tune["points"]}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, frame=frame0 + args.warmup)
     return line
@@ -402,6 +507,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="best", choices=sorted(MODES))
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-LRU comparison run")
+    ap.add_argument("--no-learned", action="store_true", help="best mode without the learned prefetch")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -192,6 +192,15 @@ vt_status vt_change_screen(vt_handle* h, int W, int H, float fovW, float fovH, f
 vt_status vt_change_num_rays(vt_handle* h, int numRayPx);
 vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], int cubeInc);
 
+/* Kernel schedule knobs of a live handle (autotuner): ray-tile shape,
+ * march unroll, persistent ray queue, traversal steps between refills,
+ * persistent CTAs per SM, lookahead requests, graph replay. */
+typedef struct {
+    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph;
+} vt_tuning;
+vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t);
+vt_status vt_get_tuning(vt_handle* h, vt_tuning* t);
+
 /* visualTur::updateVisibleCubes (src/visualTur.cu:167-228): renders the
  * current camera into dev_rgba (W*H*4 floats, pixel i*W+j) and, if not
  * NULL, dev_rgb8 (W*H*3 bytes, (uint8)(clamp(v,0,1)*255)). */
@@ -217,6 +226,11 @@ vt_status vt_get_trace(vt_handle* h, uint32_t* bits, int64_t nwords);
  * evicted.  Returns the number loaded in *loaded (may be NULL). */
 vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n, int64_t* loaded, void* stream);
 
+/* Prefetch hint for the frame after the next vt_render: during that call
+ * the bricks' host-tier reads run while its kernels render, and their
+ * device fill follows its last pass (never evicting bricks it used). */
+vt_status vt_prefetch_hint(vt_handle* h, const uint64_t* bricks, int64_t n);
+
 /* Bricks (codes at levelCubes) that hold candidate nodes of the octree,
  * sorted; n in/out: capacity / count. */
 vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n);
@@ -235,9 +249,38 @@ typedef struct {
     int64_t launches;               /* libvt kernels launched (cumulative) */
     double  ms_last_frame, ms_stall_last_frame, bytes_h2d_last_frame;
     double  ms_trace_last_frame;    /* device time of the trace kernels of the last frame */
+    double  ms_prefetch_last_frame; /* host time of the hinted prefetch's device fill */
 } vt_stats;
 vt_status vt_get_stats(vt_handle* h, vt_stats* s);
+/* Empties the brick cache (both tiers): the next frame starts cold.
+ * Synchronises the device. */
+vt_status vt_drop_cache(vt_handle* h);
 vt_status vt_reset_stats(vt_handle* h);
+
+/* ------------------------------------------------------------------------ */
+/* Learned brick prefetch (no reference counterpart)                       */
+/* ------------------------------------------------------------------------ */
+/* Multi-layer perceptron in -> h1 -> h2 -> out (ReLU, ReLU, sigmoid) with
+ * BF16 weights, FP32 master weights and FP32 accumulation; He-initialised
+ * from `seed`.  Used as pose (12 features) -> per-coarse-node probability
+ * that a frame from that pose marches the node. */
+typedef struct vt_mlp vt_mlp;
+vt_status vt_mlp_create(int in, int h1, int h2, int out, uint64_t seed, vt_mlp** m);
+void      vt_mlp_free(vt_mlp* m);
+/* probabilities of `batch` rows of dev_x (batch x in floats) into dev_p */
+vt_status vt_mlp_forward(vt_mlp* m, const float* dev_x, int batch, float* dev_p, void* stream);
+/* one Adam step on the mean binary cross-entropy against dev_y (batch x
+ * out targets in {0,1}); *loss (host, may be NULL) gets the batch loss and
+ * the call then synchronises */
+vt_status vt_mlp_train_step(vt_mlp* m, const float* dev_x, const float* dev_y, int batch, float lr,
+                            float* loss, void* stream);
+/* gradients of the batch loss without updating (host buffer laid out as
+ * the weights); synchronises */
+vt_status vt_mlp_gradients(vt_mlp* m, const float* dev_x, const float* dev_y, int batch, float* host_grads,
+                           float* loss);
+/* FP32 master weights, layer by layer: W (in x out, row-major) then b */
+vt_status vt_mlp_get_weights(vt_mlp* m, float* host, int64_t* n);
+vt_status vt_mlp_set_weights(vt_mlp* m, const float* host, int64_t n);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,92 @@
+"""Prefetch network kernels (vt_mlp_*) against a CPU FP32 implementation.
+
+The GPU forward and backward GEMMs read BF16 weights and accumulate in FP32;
+the CPU reference uses the same BF16-rounded weights in float32 numpy, so
+gradients agree up to FP32 summation order (rtol 2e-3 below)."""
+import numpy as np
+import pytest
+
+import visualtur_b200 as vt
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16(a):
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def cpu_grads(layers, x, y):
+    """mean BCE of sigmoid(relu(relu(x W1 + b1) W2 + b2) W3 + b3) and its grads"""
+    W = [bf16(w) for w, _ in layers]
+    b = [bb for _, bb in layers]
+    a0 = x
+    a1 = np.maximum(a0 @ W[0] + b[0], 0)
+    a2 = np.maximum(a1 @ W[1] + b[1], 0)
+    p = 1 / (1 + np.exp(-(a2 @ W[2] + b[2])))
+    B = x.shape[0]
+    pc = np.clip(p, 1e-7, 1 - 1e-7)
+    loss = -(y * np.log(pc) + (1 - y) * np.log(1 - pc)).sum() / B
+    d3 = (p - y) / B
+    g = [None, None, None]
+    g[2] = (a2.T @ d3, d3.sum(0))
+    d2 = (d3 @ W[2].T) * (a2 > 0)
+    g[1] = (a1.T @ d2, d2.sum(0))
+    d1 = (d2 @ W[1].T) * (a1 > 0)
+    g[0] = (a0.T @ d1, d1.sum(0))
+    return g, loss, p
+
+
+@pytest.mark.parametrize("dims,batch", [((12, 512, 512, 4096), 64), ((12, 40, 33, 70), 19)])
+def test_mlp_gradients_match_cpu(dims, batch, cuda):
+    torch = cuda
+    m = vt.MLP(dims, seed=3)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((batch, dims[0])).astype(np.float32)
+    y = (rng.random((batch, dims[3])) < 0.2).astype(np.float32)
+    dx, dy = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    layers = m.weights()
+    # He init: std sqrt(2/fan_in), zero bias
+    for l, (w, b) in enumerate(layers):
+        assert abs(w.std() / np.sqrt(2.0 / dims[l]) - 1) < 0.1 and not b.any()
+    g, loss = m.gradients(dx, dy, batch)
+    gc, lc, p = cpu_grads(layers, x.astype(np.float64).astype(np.float32), y)
+    assert abs(loss - lc) <= 1e-4 * max(1, abs(lc))
+    for (gw, gb), (cw, cb) in zip(g, gc):
+        scale = np.abs(cw).max() + 1e-12
+        assert np.abs(gw - cw).max() <= 2e-3 * scale
+        assert np.abs(gb - cb).max() <= 2e-3 * (np.abs(cb).max() + 1e-12)
+    dp = torch.empty(batch * dims[3], dtype=torch.float32, device="cuda")
+    m.forward(dx, batch, dp)
+    torch.cuda.synchronize()
+    assert np.abs(dp.cpu().numpy().reshape(batch, -1) - p).max() < 1e-4
+
+
+def test_mlp_training_reduces_loss(cuda):
+    """Learns a pose -> node-set style mapping: output k on iff a fixed
+    random projection of the input exceeds a threshold."""
+    torch = cuda
+    rng = np.random.default_rng(1)
+    n, din, dout = 4096, 12, 256
+    x = rng.standard_normal((n, din)).astype(np.float32)
+    proj = rng.standard_normal((din, dout)).astype(np.float32)
+    y = (x @ proj > 0.8).astype(np.float32)
+    m = vt.MLP((din, 128, 128, dout), seed=5)
+    dx, dy = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    first = m.train_step(dx[:256], dy[:256], 256, 2e-3)
+    for ep in range(30):
+        for i in range(0, n, 256):
+            last = m.train_step(dx[i:i + 256], dy[i:i + 256], 256, 2e-3, want_loss=False)
+    final = m.train_step(dx[:256], dy[:256], 256, 0.0)
+    assert final < 0.25 * first, (first, final)
+    # weight round trip
+    w = m.weights()
+    m2 = vt.MLP((din, 128, 128, dout), seed=6)
+    m2.set_weights(w)
+    p1 = torch.empty(256 * dout, device="cuda")
+    p2 = torch.empty(256 * dout, device="cuda")
+    m.forward(dx[:256], 256, p1)
+    m2.forward(dx[:256], 256, p2)
+    torch.cuda.synchronize()
+    assert torch.equal(p1, p2)

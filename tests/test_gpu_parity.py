@@ -34,7 +34,8 @@ def product_render(case, workdir, mode, vol=None, extra_ops=()):
         dev, host = 24, 16
     opt = vt.default_options(resident=1 if mode in ("resident", "persist") else 0, record_hits=1,
                              persistent=1 if mode in ("persist", "demand_la") else 0,
-                             lookahead=3 if mode == "demand_la" else 0, pops=3)
+                             lookahead=3 if mode == "demand_la" else 0, pops=3,
+                             unroll={"persist": 4, "demand_la": 2, "slab": 8}.get(mode, 1))
     p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=c["levelO"],
                        levelCubes=c["levelC"], dimCube=1 << (int(np.log2(c["n"])) - c["levelC"]),
                        cubeInc=c["inc"], distance=c["dist"], fov_H=c["fov"], fov_W=c["fov"],
@@ -186,7 +187,8 @@ def test_batch_parity(mode, workdir, cuda):
     dev, host = (24, 16) if mode.startswith("demand") else (512, 512)
     opt = vt.default_options(resident=1 if mode in ("resident", "persist") else 0, record_hits=0,
                              persistent=1 if mode in ("persist", "demand_la") else 0,
-                             lookahead=2 if mode == "demand_la" else 0, pops=2, tile_w=4, tile_h=4)
+                             lookahead=2 if mode == "demand_la" else 0, pops=2, tile_w=16, tile_h=16,
+                             unroll=4 if mode == "persist" else 1)
     p = vt.make_params(W=96, H=96, octreeFile=None, hdf5File=None, octreeLevel=4, levelCubes=3, dimCube=8,
                        distance=50.0, fov_H=30.0, fov_W=30.0, maxElementsCache=dev, maxElementsCache_CPU=host)
     r = vt.visualTur(p, opt, volume=fm, octree=oc)
@@ -238,3 +240,35 @@ def test_trace_log_and_prefetch(workdir, cuda):
     assert r2.prefetch(r2.brick_list()) > 0
     rgba3, _ = r2.render_host(rgb8=False)
     assert r2.stats()["passes"] == 1 and np.array_equal(rgba1, rgba3)
+
+
+def test_autotune_changes_speed_not_pixels(workdir, cuda):
+    torch = cuda
+    from visualtur_b200 import autotune as at
+    c = F.CASES["s64"]
+    vol = F.case_volume("s64")
+    fm, oc = vt.FileManager.wrap(vol), vt.Octree(F.case_octree("s64", workdir))
+    exp = oracle_render("s64", workdir)
+
+    def make(brick):
+        lc = {8: 3, 16: 2}[brick]
+        p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=4, levelCubes=lc,
+                           dimCube=brick, distance=50.0, fov_H=30.0, fov_W=30.0, maxElementsCache=512,
+                           maxElementsCache_CPU=512)
+        r = vt.visualTur(p, vt.default_options(resident=0, record_hits=1), volume=fm, octree=oc)
+        r.camera_Move(c["ops"][0][1])
+        return r
+
+    def step(r, i, stream):
+        r.updateVisibleCubes(None, stream=stream.cuda_stream)
+
+    best, table = at.tune(torch, make, step, brick_sizes=(8, 16), frames=2,
+                          tiles={32: (8, 4), 256: (16, 16)}, unrolls=(1, 4), persist=(0, 1))
+    assert len(table) == 2 * 2 * 2 * 2 and best["ms"] == min(t["ms"] for t in table)
+    for row in table[::3]:
+        r = make(row["brick"])
+        r.set_tuning(tile_w=row["tile_w"], tile_h=row["tile_h"], unroll=row["unroll"], persistent=row["persistent"])
+        rgba, rgb8 = r.render_host()
+        node = r.debug_hits()[0]
+        r.close()
+        assert np.array_equal(rgb8, exp["rgb8"]) and np.array_equal(node, exp["node"])

@@ -1,0 +1,85 @@
+"""Learned prefetch end to end on a reduced out-of-core setup.
+
+Traces of marched coarse nodes are logged by the renderer on random
+fly-throughs, the network is trained on the GPU by libvt's kernels, and a
+held-out spline fly-through is rendered with demand paging alone and with
+the network's prefetch hints.  The images must be identical frame by frame
+(a prediction never changes a pixel) and the learned hints must raise the
+device-cache hit rate and cut the demand passes."""
+import numpy as np
+import pytest
+
+import visualtur_b200 as vt
+from visualtur_b200 import prefetch as pf
+
+pytestmark = pytest.mark.gpu
+
+N, ISO, LC, LO, LEVEL = 256, 0.6, 4, 6, 3
+W, H, FOV = 96, 72, 30.0
+
+
+@pytest.fixture(scope="module")
+def scene(tmp_path_factory):
+    d = tmp_path_factory.mktemp("pf")
+    vol = vt.generate_volume(vt.VT_GEN_BLOBS, 17, (N, N, N), (48, 6.0, 24.0, 0.5, 1.5, 0.05))
+    path = str(d / "blobs.oct")
+    vt.build_octree(vt.FileManager.wrap(vol), ISO, path)
+    return vol, path
+
+
+def make(vol, path, dev_slots, host_slots, **opt):
+    fm, oc = vt.FileManager.wrap(vol), vt.Octree(path)
+    p = vt.make_params(W=W, H=H, octreeFile=None, hdf5File=None, octreeLevel=LO, levelCubes=LC, dimCube=16,
+                       distance=50.0, fov_H=FOV, fov_W=FOV, maxElementsCache=dev_slots,
+                       maxElementsCache_CPU=host_slots)
+    return vt.visualTur(p, vt.default_options(**opt), volume=fm, octree=oc), (fm, oc)
+
+
+def test_learned_prefetch_gains_over_demand_paging(scene, cuda):
+    torch = cuda
+    vol, path = scene
+    # traces from random fly-throughs (resident renderer with the access log)
+    tr, keep = make(vol, path, 8 ** LC, 8 ** LC, resident=1, record_trace=1, trace_level=LEVEL, record_hits=0)
+    rng = np.random.default_rng(123)
+    X, Y = [], []
+    for path_i in range(20):
+        pos, tgt = pf.random_flythrough(rng, N, 60, 1.2 * N, 1.8 * N)
+        for p_, t_ in zip(pos, tgt):
+            cam = pf.look_at(W, H, 50.0, FOV, p_, t_)
+            tr.set_camera(cam)
+            tr.render_host(rgb8=False)
+            X.append(pf.pose_features(cam, N, FOV))
+            Y.append(pf.trace_to_targets(tr.trace(LEVEL), LEVEL))
+    X, Y = np.array(X), np.array(Y)
+    assert 0.02 < Y.mean() < 0.9
+    bricks = tr.brick_list()
+    P = pf.Prefetcher(N, FOV, LC, bricks, seed=1, hidden=128, level=LEVEL)
+    hist = P.train(torch, X, Y, epochs=40, batch=128, lr=2e-3)
+    assert hist[-1] < 0.6 * hist[0]
+
+    # held-out spline; device cache holds a quarter of the bricks
+    pos, tgt = pf.random_flythrough(np.random.default_rng(999), N, 60, 1.3 * N, 1.7 * N)
+    cams = [pf.look_at(W, H, 50.0, FOV, p_, t_) for p_, t_ in zip(pos, tgt)]
+    dev = max(64, len(bricks) // 4)
+    results = {}
+    for mode in ("demand", "learned"):
+        r, keep2 = make(vol, path, dev, len(bricks), resident=0, preload=0, record_hits=0)
+        imgs, passes = [], []
+        if mode == "learned":
+            r.prefetch(P.bricks_for(P.predict(torch, pf.pose_features(cams[0], N, FOV))[0], 0.3))
+        for k, cam in enumerate(cams):
+            if mode == "learned" and k + 1 < len(cams):
+                probs = P.predict(torch, pf.pose_features(cams[k + 1], N, FOV))[0]
+                r.prefetch_hint(P.bricks_for(probs, 0.3))
+            r.set_camera(cam)
+            rgba, _ = r.render_host(rgb8=False)
+            imgs.append(rgba)
+            passes.append(r.stats()["passes"])
+        s = r.stats()
+        hit_rate = s["device_hits"] / max(1, s["device_hits"] + s["device_misses"])
+        results[mode] = dict(imgs=imgs, passes=np.mean(passes), hit_rate=hit_rate, stats=s)
+        r.close()
+    for a, b in zip(results["demand"]["imgs"], results["learned"]["imgs"]):
+        assert np.array_equal(a, b)
+    assert results["learned"]["hit_rate"] > results["demand"]["hit_rate"]
+    assert results["learned"]["passes"] < results["demand"]["passes"]

@@ -55,7 +55,15 @@ class vt_stats(C.Structure):
         "bricks_requested", "bricks_loaded_host", "bricks_loaded_disk", "bricks_prefetched",
         "device_hits", "device_misses", "host_hits", "host_misses", "max_stack", "launches")] + \
         [(n, C.c_double) for n in ("ms_last_frame", "ms_stall_last_frame", "bytes_h2d_last_frame",
-                                   "ms_trace_last_frame")]
+                                   "ms_trace_last_frame", "ms_prefetch_last_frame")]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class vt_tuning(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("tile_w", "tile_h", "unroll", "persistent", "pops", "blocks_per_sm",
+                                         "lookahead", "use_graph")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -108,8 +116,19 @@ _PROTOS = {
     "vt_get_trace": (C.c_int, [_P, _P, C.c_int64]),
     "vt_prefetch": (C.c_int, [_P, _P, C.c_int64, C.POINTER(C.c_int64), _P]),
     "vt_brick_list": (C.c_int, [_P, _P, C.POINTER(C.c_int64)]),
+    "vt_prefetch_hint": (C.c_int, [_P, _P, C.c_int64]),
+    "vt_set_tuning": (C.c_int, [_P, C.POINTER(vt_tuning)]),
+    "vt_drop_cache": (C.c_int, [_P]),
+    "vt_get_tuning": (C.c_int, [_P, C.POINTER(vt_tuning)]),
     "vt_get_stats": (C.c_int, [_P, C.POINTER(vt_stats)]),
     "vt_reset_stats": (C.c_int, [_P]),
+    "vt_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_P)]),
+    "vt_mlp_free": (None, [_P]),
+    "vt_mlp_forward": (C.c_int, [_P, _P, C.c_int, _P, _P]),
+    "vt_mlp_train_step": (C.c_int, [_P, _P, _P, C.c_int, C.c_float, C.POINTER(C.c_float), _P]),
+    "vt_mlp_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, C.POINTER(C.c_float)]),
+    "vt_mlp_get_weights": (C.c_int, [_P, _P, C.POINTER(C.c_int64)]),
+    "vt_mlp_set_weights": (C.c_int, [_P, _P, C.c_int64]),
 }
 
 _lib = None
@@ -405,6 +424,7 @@ class visualTur:
         check(lib().vt_change_cache(self._h, nE, _i3(cDim), cInc))
 
     def updateVisibleCubes(self, dev_rgba, dev_rgb8=None, stream=None):
+        """Renders into caller device buffers (both None: the handle's own)."""
         check(lib().vt_render(self._h, _ptr(dev_rgba), _ptr(dev_rgb8), stream))
 
     def render_host(self, rgb8=True):
@@ -438,6 +458,22 @@ class visualTur:
         check(lib().vt_prefetch(self._h, b.ctypes.data, int(b.size), C.byref(got), stream))
         return got.value
 
+    def tuning(self):
+        t = vt_tuning()
+        check(lib().vt_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = vt_tuning()
+        check(lib().vt_get_tuning(self._h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        check(lib().vt_set_tuning(self._h, C.byref(t)))
+
+    def prefetch_hint(self, bricks):
+        b = np.ascontiguousarray(bricks, np.uint64)
+        check(lib().vt_prefetch_hint(self._h, b.ctypes.data if b.size else None, int(b.size)))
+
     def brick_list(self):
         n = C.c_int64(0)
         check(lib().vt_brick_list(self._h, None, C.byref(n)))
@@ -453,9 +489,69 @@ class visualTur:
     def reset_stats(self):
         check(lib().vt_reset_stats(self._h))
 
+    def drop_cache(self):
+        check(lib().vt_drop_cache(self._h))
+
     def close(self):
         if self._h:
             lib().vt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MLP:
+    """Prefetch network (vt_mlp_*): in -> h1 -> h2 -> out, BF16 weights, FP32
+    accumulation, trained on the GPU by libvt's own kernels."""
+
+    def __init__(self, dims=(12, 512, 512, 4096), seed=0):
+        self.dims = tuple(int(d) for d in dims)
+        self._h = C.c_void_p()
+        check(lib().vt_mlp_create(*self.dims, seed, C.byref(self._h)))
+
+    def forward(self, dev_x, batch, dev_p, stream=None):
+        check(lib().vt_mlp_forward(self._h, _ptr(dev_x), batch, _ptr(dev_p), stream))
+
+    def train_step(self, dev_x, dev_y, batch, lr, stream=None, want_loss=True):
+        loss = C.c_float()
+        check(lib().vt_mlp_train_step(self._h, _ptr(dev_x), _ptr(dev_y), batch, lr,
+                                      C.byref(loss) if want_loss else None, stream))
+        return loss.value
+
+    def gradients(self, dev_x, dev_y, batch):
+        n = C.c_int64(0)
+        check(lib().vt_mlp_get_weights(self._h, None, C.byref(n)))
+        g = np.empty(n.value, np.float32)
+        loss = C.c_float()
+        check(lib().vt_mlp_gradients(self._h, _ptr(dev_x), _ptr(dev_y), batch, g.ctypes.data, C.byref(loss)))
+        return self._split(g), loss.value
+
+    def weights(self):
+        n = C.c_int64(0)
+        check(lib().vt_mlp_get_weights(self._h, None, C.byref(n)))
+        w = np.empty(n.value, np.float32)
+        check(lib().vt_mlp_get_weights(self._h, w.ctypes.data, C.byref(n)))
+        return self._split(w)
+
+    def set_weights(self, layers):
+        flat = np.concatenate([np.ascontiguousarray(a, np.float32).ravel() for wb in layers for a in wb])
+        check(lib().vt_mlp_set_weights(self._h, flat.ctypes.data, flat.size))
+
+    def _split(self, flat):
+        out, o, d = [], 0, self.dims
+        for l in range(3):
+            nw = d[l] * d[l + 1]
+            out.append((flat[o:o + nw].reshape(d[l], d[l + 1]), flat[o + nw:o + nw + d[l + 1]]))
+            o += nw + d[l + 1]
+        return out
+
+    def close(self):
+        if self._h:
+            lib().vt_mlp_free(self._h)
             self._h = None
 
     def __del__(self):

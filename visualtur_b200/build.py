@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libvt.so")
 BUILD = os.path.join(ROOT, "_build", "vt")
 
-CU = ["render.cu", "cache.cu", "gen.cu", "builder.cu"]
+CU = ["render.cu", "cache.cu", "gen.cu", "builder.cu", "mlp.cu"]
 CPP = ["volume.cpp", "octree.cpp", "runtime.cpp", "h5lite.cpp"]
 
 

@@ -240,24 +240,46 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
     return st;
 }
 
-vt_status BrickCache::prefetch(const std::vector<uint64_t>& bricks, cudaStream_t s, int64_t* loaded) {
-    std::vector<uint64_t> want;
-    for (uint64_t b : bricks)
-        if (pageMirror_[b - pageBase_] < 0) want.push_back(b);
-    size_t cap = std::min<size_t>({want.size(), (size_t)nSlots_, (size_t)nHost_});
-    want.resize(cap);
-    if (want.empty()) return VT_OK;
-    std::vector<int> hs;
+vt_status BrickCache::prefetch_stage(const std::vector<uint64_t>& bricks, std::vector<uint64_t>& staged,
+                                      std::vector<int>& hslot) {
+    staged.clear();
+    const size_t cap = (size_t)std::min(nSlots_, nHost_);
+    for (uint64_t b : bricks) {
+        if (staged.size() >= cap) break;
+        if (pageMirror_[b - pageBase_] < 0) staged.push_back(b);
+    }
+    if (staged.empty()) { hslot.clear(); return VT_OK; }
     int64_t disk = 0;
-    vt_status st = ensure_host(want, hs, &disk);
-    if (st != VT_OK) return st;
+    return ensure_host(staged, hslot, &disk);
+}
+
+vt_status BrickCache::prefetch_commit(const std::vector<uint64_t>& staged, const std::vector<int>& hslot,
+                                      cudaStream_t s, int64_t* loaded) {
+    std::vector<uint64_t> b;
+    std::vector<int> hs;
+    for (size_t i = 0; i < staged.size(); i++) {
+        /* skip bricks demand paging loaded meanwhile, or whose host copy was evicted */
+        if (pageMirror_[staged[i] - pageBase_] >= 0 || hslot[i] < 0) continue;
+        if (hostIndex_[staged[i] - pageBase_] != hslot[i]) continue;
+        b.push_back(staged[i]);
+        hs.push_back(hslot[i]);
+    }
+    if (b.empty()) return VT_OK;
     double h2d = 0;
     int64_t got = 0;
     /* never evict a slot used since the frame began */
-    st = assign_device(want, hs, s, frameStart_, &h2d, &got);
+    vt_status st = assign_device(b, hs, s, frameStart_, &h2d, &got);
     prefetched_ += got;
     if (loaded) *loaded += got;
     return st;
+}
+
+vt_status BrickCache::prefetch(const std::vector<uint64_t>& bricks, cudaStream_t s, int64_t* loaded) {
+    std::vector<uint64_t> staged;
+    std::vector<int> hs;
+    vt_status st = prefetch_stage(bricks, staged, hs);
+    if (st != VT_OK) return st;
+    return prefetch_commit(staged, hs, s, loaded);
 }
 
 vt_status BrickCache::preload(const std::vector<uint64_t>& bricks) {
@@ -284,6 +306,20 @@ void BrickCache::fold_stats(vt_stats& st) {
     st.launches += launches_ - launchesFolded_;
     launchesFolded_ = launches_;
 }
+vt_status BrickCache::drop() {
+    CKC(cudaDeviceSynchronize());
+    CKC(cudaMemset(d_page_, 0xFF, pageN_ * 4));
+    CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
+    std::fill(slotBrick_.begin(), slotBrick_.end(), 0);
+    std::fill(stampHost_.begin(), stampHost_.end(), 0);
+    std::fill(pageMirror_.begin(), pageMirror_.end(), -1);
+    std::fill(hostIndex_.begin(), hostIndex_.end(), -1);
+    std::fill(hostBrick_.begin(), hostBrick_.end(), 0);
+    std::fill(hostTick_.begin(), hostTick_.end(), 0);
+    allResident_ = false;
+    return VT_OK;
+}
+
 void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = 0; }
 
 }  // namespace vtrt

@@ -45,7 +45,15 @@ public:
     /* loads bricks ahead of demand (prefetch); never evicts slots stamped
      * in the current frame */
     vt_status prefetch(const std::vector<uint64_t>& bricks, cudaStream_t s, int64_t* loaded);
+    /* the two halves of prefetch: host-tier loads (no device work, may run
+     * while a frame's kernels are in flight) and the device fill */
+    vt_status prefetch_stage(const std::vector<uint64_t>& bricks, std::vector<uint64_t>& staged,
+                             std::vector<int>& hslot);
+    vt_status prefetch_commit(const std::vector<uint64_t>& staged, const std::vector<int>& hslot, cudaStream_t s,
+                              int64_t* loaded);
     void fold_stats(vt_stats& st);
+    /* empties both tiers (cold cache); no kernel may be in flight */
+    vt_status drop();
     void reset_stats();
     int device_slots() const { return nSlots_; }
     size_t slot_bytes() const { return slotBytes_; }

@@ -68,8 +68,12 @@ __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
 
 /* The march of cuda_rayCaster (src/rayCaster.cu:166-237): samples at
  * Xnear, Xnear += 0.5*dir, for steps 0..maxStep; the first sign change of
- * iso - value (equality counts) is refined once linearly. */
-template <int VTYPE>
+ * iso - value (equality counts) is refined once linearly.  U samples are
+ * fetched per round: their positions accumulate in the reference's order,
+ * their taps are issued together, and the crossing test then runs sample
+ * by sample -- fetches past the hit are discarded (indices stay clamped to
+ * the brick) and are not counted. */
+template <int VTYPE, int U>
 __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, float tnear,
                                       int maxStep, float iso, float3* Xhit, unsigned int* nsamp) {
     float3 Xnear = add(origin, mul(ray, tnear));
@@ -79,20 +83,29 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
     float ant = interp<VTYPE>(s, Xnear);
     unsigned int ns = 1;
     bool hit = false;
-    for (int steps = 1; steps <= maxStep; steps++) {
-        Xnear = add(Xnear, vStep);
-        float sig = interp<VTYPE>(s, Xnear);
-        ns++;
-        if ((((iso - ant) < 0.0f) && ((iso - sig) < 0.0f)) ||
-            (((iso - ant) > 0.0f) && ((iso - sig) > 0.0f))) {
-            ant = sig;
-            Xfar = Xnear;
-        } else {
-            float a = (iso - ant) / (sig - ant);
-            *Xhit = add(mul(Xfar, 1.0f - a), mul(Xnear, a));
-            hit = true;
-            break;
+    for (int steps = 1; steps <= maxStep && !hit; steps += U) {
+        float3 X[U];
+        float v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) X[u] = add(u == 0 ? Xnear : X[u - 1], vStep);
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = interp<VTYPE>(s, X[u]);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (hit || steps + u > maxStep) break;
+            float sig = v[u];
+            ns++;
+            if ((((iso - ant) < 0.0f) && ((iso - sig) < 0.0f)) ||
+                (((iso - ant) > 0.0f) && ((iso - sig) > 0.0f))) {
+                ant = sig;
+                Xfar = X[u];
+            } else {
+                float a = (iso - ant) / (sig - ant);
+                *Xhit = add(mul(Xfar, 1.0f - a), mul(X[u], a));
+                hit = true;
+            }
         }
+        Xnear = X[U - 1];
     }
     *nsamp += ns;
     return hit;
@@ -159,7 +172,7 @@ __device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned long 
  * ray is shaded or exhausted, RAY_SUSPENDED when its next candidate's brick
  * is not resident (the candidate stays on the stack), RAY_RUNNING when the
  * budget ran out. */
-template <int VTYPE, bool SLAB>
+template <int VTYPE, bool SLAB, int U>
 __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, int budget) {
     const DevOctree& O = A.oct;
     const int nLevels = O.nLevels, Lo = O.Lo;
@@ -195,7 +208,7 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
             if (!slab(R.r, mb.x, mb.y, mb.z, mb.x + dimO, mb.y + dimO, mb.z + dimO, &tn, &tf)) continue;
             float3 X;
             unsigned int ns = 0;
-            bool h = march<VTYPE>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
+            bool h = march<VTYPE, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
             cnt[VT_C_SAMPLES] += ns;
             if (h) {
                 /* shade (src/rayCaster.cu:238-250) */
@@ -222,12 +235,26 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
         float ctn[8], ctf[8];
         int nv = 0;
         unsigned int m = nd.y;
+        /* the children's faces lie on 3 planes per axis: the slab products
+         * of all 8 children are these 9 values (the same float operations
+         * the reference performs per child, src/Octree.cu:258-330) */
+        const float x0 = ((float)mb.x - R.r.o.x) * R.r.dx, x1 = ((float)(mb.x + cd) - R.r.o.x) * R.r.dx,
+                    x2 = ((float)(mb.x + 2 * cd) - R.r.o.x) * R.r.dx;
+        const float y0 = ((float)mb.y - R.r.o.y) * R.r.dy, y1 = ((float)(mb.y + cd) - R.r.o.y) * R.r.dy,
+                    y2 = ((float)(mb.y + 2 * cd) - R.r.o.y) * R.r.dy;
+        const float z0 = ((float)mb.z - R.r.o.z) * R.r.dz, z1 = ((float)(mb.z + cd) - R.r.o.z) * R.r.dz,
+                    z2 = ((float)(mb.z + 2 * cd) - R.r.o.z) * R.r.dz;
+        const bool px = R.r.dx >= 0, py = R.r.dy >= 0, pz = R.r.dz >= 0;
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             if ((m >> k) & 1u) {
-                int bx = mb.x + ((k >> 2) & 1) * cd, by = mb.y + ((k >> 1) & 1) * cd, bz = mb.z + (k & 1) * cd;
+                const int kx = (k >> 2) & 1, ky = (k >> 1) & 1, kz = k & 1;
+                const float xa = kx ? x1 : x0, xb = kx ? x2 : x1;
+                const float ya = ky ? y1 : y0, yb = ky ? y2 : y1;
+                const float za = kz ? z1 : z0, zb = kz ? z2 : z1;
                 float a, b;
-                if (slab(R.r, bx, by, bz, bx + cd, by + cd, bz + cd, &a, &b) && b >= 0.0f) {
+                if (slab_t(px ? xa : xb, px ? xb : xa, py ? ya : yb, py ? yb : ya, pz ? za : zb, pz ? zb : za, &a, &b) &&
+                    b >= 0.0f) {
                     unsigned long long cidx = nd.x + __popc(m & ((1u << k) - 1u));
                     cent[nv] = (cidx << codeBits) | ((code << 3) + (unsigned long long)k);
                     ctn[nv] = a; ctf[nv] = b;
@@ -412,7 +439,7 @@ __device__ __forceinline__ void flush_counters(const TraceArgs& A, unsigned int*
  * keeps its 32 lanes busy, and after every `pops` traversal steps the lanes
  * whose ray finished or suspended take new work items -- a ballot of the
  * idle lanes, one atomicAdd by the leader, and a popcount rank per lane. */
-template <int VTYPE, bool SLAB, bool PERSIST>
+template <int VTYPE, bool SLAB, bool PERSIST, int U>
 __global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
     __shared__ DevView sv[VT_MAX_VIEWS];
     for (int k = threadIdx.x; k < A.views.n; k += blockDim.x) sv[k] = A.views.v[k];
@@ -427,7 +454,7 @@ __global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
         unsigned int w = blockIdx.x * blockDim.x + threadIdx.x;
         if (w < nItems) {
             int s = start_ray<VTYPE>(A, sv, w, R, st, cnt);
-            if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB>(A, R, st, cnt, -1);
+            if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB, U>(A, R, st, cnt, -1);
             if (s == RAY_DONE) write_ray(A, sv, R, cnt);
             else if (s == RAY_SUSPENDED) suspend_ray<VTYPE, SLAB>(A, R, st, cnt);
         }
@@ -452,7 +479,7 @@ __global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
                 }
             }
             if (has) {
-                int s = run_ray<VTYPE, SLAB>(A, R, st, cnt, A.pops);
+                int s = run_ray<VTYPE, SLAB, U>(A, R, st, cnt, A.pops);
                 if (s == RAY_DONE) { write_ray(A, sv, R, cnt); has = false; }
                 else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB>(A, R, st, cnt); has = false; }
             }
@@ -585,14 +612,22 @@ cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, bool persistent, 
     } else {
         blocks = (items + threads - 1) / threads;
     }
-#define VT_LAUNCH(V, S, P) k_trace<V, S, P><<<blocks, threads, 0, s>>>(a)
-    if (a.br.vtype == 0) {
-        if (slabMode) { if (persistent) VT_LAUNCH(0, true, true); else VT_LAUNCH(0, true, false); }
-        else { if (persistent) VT_LAUNCH(0, false, true); else VT_LAUNCH(0, false, false); }
-    } else {
-        if (slabMode) { if (persistent) VT_LAUNCH(1, true, true); else VT_LAUNCH(1, true, false); }
-        else { if (persistent) VT_LAUNCH(1, false, true); else VT_LAUNCH(1, false, false); }
+#define VT_LAUNCH_U(V, S, P)                                            \
+    switch (a.unroll) {                                                 \
+        case 2: k_trace<V, S, P, 2><<<blocks, threads, 0, s>>>(a); break; \
+        case 4: k_trace<V, S, P, 4><<<blocks, threads, 0, s>>>(a); break; \
+        case 8: k_trace<V, S, P, 8><<<blocks, threads, 0, s>>>(a); break; \
+        default: k_trace<V, S, P, 1><<<blocks, threads, 0, s>>>(a); break; \
     }
+#define VT_LAUNCH(V, S, P) VT_LAUNCH_U(V, S, P)
+    if (a.br.vtype == 0) {
+        if (slabMode) { if (persistent) VT_LAUNCH(0, true, true) else VT_LAUNCH(0, true, false) }
+        else { if (persistent) VT_LAUNCH(0, false, true) else VT_LAUNCH(0, false, false) }
+    } else {
+        if (slabMode) { if (persistent) VT_LAUNCH(1, true, true) else VT_LAUNCH(1, true, false) }
+        else { if (persistent) VT_LAUNCH(1, false, true) else VT_LAUNCH(1, false, false) }
+    }
+#undef VT_LAUNCH_U
 #undef VT_LAUNCH
     return cudaGetLastError();
 }

@@ -181,6 +181,7 @@ struct vt_handle {
     std::vector<cudaEvent_t> ev;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t s_int = nullptr;
+    std::vector<uint64_t> hint;            /* bricks to load for the next frame */
     vt_stats stats;
     bool lastValid = false;
 };
@@ -323,7 +324,9 @@ static vt_status validate(const vt_params* p, const vt_octree* o, const vt_optio
     if (p->cubeInc < 3) return fail(VT_ERR_INVALID, "cubeInc must be >= 3 so every trilinear and normal tap stays in the brick");
     if (opt) {
         int tw = opt->tile_w, th = opt->tile_h;
-        if (tw <= 0 || th <= 0 || tw * th > 128 || 128 % (tw * th)) return fail(VT_ERR_INVALID, "tile %dx%d must divide 128 rays", tw, th);
+        if (tw <= 0 || th <= 0 || tw * th > 4096) return fail(VT_ERR_INVALID, "tile %dx%d: 1..4096 rays", tw, th);
+        if (opt->unroll != 1 && opt->unroll != 2 && opt->unroll != 4 && opt->unroll != 8)
+            return fail(VT_ERR_INVALID, "unroll must be 1, 2, 4 or 8");
         if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
             return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
     }
@@ -502,6 +505,7 @@ static void fill_args(vt_handle* h, TraceArgs& a, int nViews, unsigned int total
     a.light = make_float3(0.0f, 512.0f, 0.0f);   /* src/visualTur.cu:30 */
     a.tile_w = h->opt.tile_w; a.tile_h = h->opt.tile_h;
     a.pops = h->opt.pops > 0 ? h->opt.pops : 8;
+    a.unroll = h->opt.unroll;
 }
 
 static vt_status collect_counters(vt_handle* h, cudaStream_t s) {
@@ -602,6 +606,13 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
     h->stats.launches++;
     int passes = 1;
     double stall = 0, h2d = 0;
+    /* prefetch hint for the next frame: host-tier loads overlap this frame's kernel */
+    std::vector<uint64_t> staged;
+    std::vector<int> stagedSlots;
+    if (slabMode && !h->hint.empty()) {
+        if ((st = h->cache->prefetch_stage(h->hint, staged, stagedSlots)) != VT_OK) return st;
+        h->hint.clear();
+    }
     if (!allResident) {
         int cur = 0;
         for (;;) {
@@ -628,6 +639,16 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
         }
     }
     if ((st = collect_counters(h, s)) != VT_OK) return st;
+    if (!staged.empty()) {
+        auto tp = std::chrono::steady_clock::now();
+        int64_t got = 0;
+        if ((st = h->cache->prefetch_commit(staged, stagedSlots, s, &got)) != VT_OK) return st;
+        CK(cudaStreamSynchronize(s));
+        h->stats.ms_prefetch_last_frame =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count();
+    } else {
+        h->stats.ms_prefetch_last_frame = 0;
+    }
     double tk = 0;
     for (int k = 0; k < passes; k++) {
         float ms = 0;
@@ -720,6 +741,41 @@ extern "C" vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n
     return s;
 }
 
+extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
+    clear_error();
+    if (!h || !t) return fail(VT_ERR_INVALID, "null argument");
+    vt_options o = h->opt;
+    o.tile_w = t->tile_w; o.tile_h = t->tile_h; o.unroll = t->unroll; o.persistent = t->persistent;
+    o.pops = t->pops; o.blocks_per_sm = t->blocks_per_sm; o.lookahead = t->lookahead; o.use_graph = t->use_graph;
+    vt_status s = validate(&h->p, h->oct, &o);
+    if (s != VT_OK) return s;
+    if (o.lookahead < 0 || o.lookahead > 64 || o.pops < 1 || o.blocks_per_sm < 1 || o.blocks_per_sm > 32)
+        return fail(VT_ERR_INVALID, "lookahead 0..64, pops >= 1, blocks_per_sm 1..32");
+    h->opt = o;
+    return VT_OK;
+}
+
+extern "C" vt_status vt_get_tuning(vt_handle* h, vt_tuning* t) {
+    clear_error();
+    if (!h || !t) return fail(VT_ERR_INVALID, "null argument");
+    t->tile_w = h->opt.tile_w; t->tile_h = h->opt.tile_h; t->unroll = h->opt.unroll; t->persistent = h->opt.persistent;
+    t->pops = h->opt.pops; t->blocks_per_sm = h->opt.blocks_per_sm; t->lookahead = h->opt.lookahead;
+    t->use_graph = h->opt.use_graph;
+    return VT_OK;
+}
+
+extern "C" vt_status vt_prefetch_hint(vt_handle* h, const uint64_t* bricks, int64_t n) {
+    clear_error();
+    if (!h || (!bricks && n > 0)) return fail(VT_ERR_INVALID, "null argument");
+    uint64_t lo = 1ull << (3 * h->Lc), hi = lo << 3;
+    h->hint.clear();
+    for (int64_t i = 0; i < n; i++) {
+        if (bricks[i] < lo || bricks[i] >= hi) return fail(VT_ERR_INVALID, "brick code %llu not at levelCubes", (unsigned long long)bricks[i]);
+        h->hint.push_back(bricks[i]);
+    }
+    return VT_OK;
+}
+
 extern "C" vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n) {
     clear_error();
     if (!h || !n) return fail(VT_ERR_INVALID, "null argument");
@@ -727,6 +783,14 @@ extern "C" vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n) {
     *n = (int64_t)h->leafBricks.size();
     if (bricks) memcpy(bricks, h->leafBricks.data(), (size_t)std::min<int64_t>(cap, *n) * 8);
     return VT_OK;
+}
+
+extern "C" vt_status vt_drop_cache(vt_handle* h) {
+    clear_error();
+    if (!h) return fail(VT_ERR_INVALID, "null handle");
+    h->hint.clear();
+    if (!h->cache) return VT_OK;
+    return h->cache->drop();
 }
 
 extern "C" vt_status vt_get_stats(vt_handle* h, vt_stats* s) {

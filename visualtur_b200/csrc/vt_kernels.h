@@ -103,6 +103,7 @@ struct TraceArgs {
     float3 light;
     int tile_w, tile_h;
     int pops;                                   /* pops between warp refills (persistent) */
+    int unroll;                                 /* march samples fetched per round: 1, 2, 4, 8 */
 };
 
 /* launchers (render.cu) */

@@ -64,6 +64,22 @@ __device__ __forceinline__ bool slab(const RayInv& r, int mnx, int mny, int mnz,
     return hit;
 }
 
+/* The comparison half of slab(): per-axis entry/exit parameters already
+ * ordered by the direction's sign.  slab() == slab_t() on the same planes. */
+__device__ __forceinline__ bool slab_t(float tmin, float tmax, float tymin, float tymax, float tzmin, float tzmax,
+                                       float* tnear, float* tfar) {
+    bool hit = true;
+    if ((tmin > tymax) || (tymin > tmax)) hit = false;
+    if (tymin > tmin) tmin = tymin;
+    if (tymax < tmax) tmax = tymax;
+    if ((tmin > tzmax) || (tzmin > tmax)) hit = false;
+    if (tzmin > tmin) tmin = tzmin;
+    if (tzmax < tmax) tmax = tzmax;
+    *tnear = (tmin < 0.0f) ? 0.0f : tmin;
+    *tfar = tmax;
+    return hit;
+}
+
 /* Level of a sentinel-bit Morton code (getIndexLevel,
  * inc/mortonCodeUtil.hpp:42-86) for valid codes (>= 1). */
 __device__ __forceinline__ int code_level(uint64_t c) { return (63 - __clzll((long long)c)) / 3; }
