@@ -44,7 +44,7 @@ CONFIGS = {
                gen="sphere", seed=1234, n=128, iso=40.0, levelC=4, levelO=5, inc=3, W=512, H=512, fov=30.0,
                dist=50.0, resident=1, l2flush=True, orbit=None, cam_pos=(63.5, 63.5, 363.5)),
     "c2": dict(workload="2048^3 f32 blobs+noise, iso 0.6, out-of-core: 16^3 bricks (apron 3), 4 GB device "
-                        "cache, 16 GB pinned host tier, 1920x1080, orbit r=3000 at 1.2 deg/frame from a cold cache",
+                        "cache, 16 GB pinned host tier, 1920x1080, orbit r=3000 at 1.2 deg/frame, timed from a cold cache",
                gen="blobs", seed=2048, n=2048, iso=0.6, levelC=7, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
                dist=50.0, resident=0, l2flush=False, orbit=(3000.0, 1.2), dev_bytes=4 << 30,
                host_bytes=16 << 30, blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05)),
@@ -138,7 +138,7 @@ def frame_camera(vt, cfg, frame):
 class Workload:
     """Volume (device generated), octree (GPU builder) and renderer."""
 
-    def __init__(self, cfg, torch, device, workdir, need_renderer=True, mode="best"):
+    def __init__(self, cfg, torch, device, workdir, need_renderer=True, mode="best", warm=False):
         import visualtur_b200 as vt
         self.vt, self.cfg = vt, cfg
         n = cfg["n"]
@@ -178,14 +178,15 @@ class Workload:
                                fov_H=cfg["fov"], fov_W=cfg["fov"], maxElementsCache=dev, maxElementsCache_CPU=host)
             self.params = p
             t4 = time.time()
-            self.r = self.renderer(mode)
+            self.r = self.renderer(mode, warm)
             log("setup: renderer %.1fs (device slots %d, host slots %d, %d B/brick)" % (time.time() - t4, dev, host, slot))
 
 
-    def renderer(self, mode):
-        """A renderer in `mode` (cold cache unless the workload is resident)."""
+    def renderer(self, mode, warm=False):
+        """A renderer in `mode` (cold cache unless the workload is resident
+        or `warm`: every needed brick preloaded, for steady-state profiles)."""
         opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=0,
-                                      preload=1 if self.cfg["resident"] else 0, **MODES[mode]["opts"])
+                                      preload=1 if (self.cfg["resident"] or warm) else 0, **MODES[mode]["opts"])
         return self.vt.visualTur(self.params, opt, volume=self.fm, octree=self.oc)
 
     def train_prefetcher(self, torch, poses=20000, paths=100, W=240, H=135, epochs=30):
@@ -276,8 +277,9 @@ class Launcher:
     """Renders consecutive orbit frames in launches of `batch` views; with a
     predictor, hands the renderer the predicted bricks of the next launch."""
 
-    def __init__(self, wl, r, cfg, torch, dev, stream, batch=1, predictor=None, threshold=0.25):
+    def __init__(self, wl, r, cfg, torch, dev, stream, batch=1, predictor=None, threshold=0.25, warm=False):
         self.wl, self.r, self.cfg, self.torch, self.stream = wl, r, cfg, torch, stream
+        self.warm = warm
         self.batch, self.P, self.thr = batch, predictor, threshold
         W, H = cfg["W"], cfg["H"]
         self.bufs = [(torch.empty(W * H * 4, dtype=torch.float32, device=dev),
@@ -323,6 +325,8 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
             L.launch(L.cams(f, n), L.cams(f + n, nxt))
             f += n
         torch.cuda.synchronize()
+        if not L.cfg["resident"] and not L.warm:
+            r.drop_cache()     # every timed run starts from a cold cache: all loading is timed
         r.reset_stats()
         launches = []
         f = frame0 + warmup
@@ -365,7 +369,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     torch.cuda.set_device(dev)
     work = tempfile.mkdtemp(prefix="vtbench_")
     M = MODES[args.mode]
-    wl = Workload(cfg, torch, dev, work, mode=args.mode)
+    wl = Workload(cfg, torch, dev, work, mode=args.mode, warm=args.warm)
     W, H = cfg["W"], cfg["H"]
     stream = torch.cuda.Stream(device=dev)
     frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
@@ -380,8 +384,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
         tune = {"best": best, "points": len(table), "table": table}
         log("autotune: best %s" % best)
         if not cfg["resident"]:
-            wl.r.drop_cache()     # the timed run starts from a cold cache
-    L = Launcher(wl, wl.r, cfg, torch, dev, stream, batch=batch, predictor=P)
+            wl.r.drop_cache()
+    L = Launcher(wl, wl.r, cfg, torch, dev, stream, batch=batch, predictor=P, warm=args.warm)
     ms, per, nfr, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index), cfg["l2flush"])
     tot_ms = sum(ms)
     st = wl.r.stats()
@@ -509,6 +513,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-LRU comparison run")
     ap.add_argument("--no-learned", action="store_true", help="best mode without the learned prefetch")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--warm", action="store_true", help="profiling: preloaded cache, no cold start")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -64,8 +64,8 @@ vt_status BrickCache::init(const CacheConfig& c) {
     D_ = c.edge + 2 * c.inc;
     slotBytes_ = ((size_t)D_ * D_ * D_ * esize_ + 15) & ~(size_t)15;
     brickVol_ = slotBytes_ / esize_;
-    pageBase_ = 1ull << (3 * c.Lc);
-    pageN_ = (size_t)pageBase_;
+    pageBase_ = 0;                     /* keys are page indices (bx << 2Lc | by << Lc | bz) */
+    pageN_ = (size_t)1 << (3 * c.Lc);
     nSlots_ = c.deviceSlots;
     nHost_ = c.hostSlots;
     CKC(cudaMalloc(&d_page_, pageN_ * 4));
@@ -89,8 +89,10 @@ void BrickCache::fill_args(DevBricks& b) const {
     b.inc = cfg_.inc; b.vtype = cfg_.vol->vtype; b.stamp = d_stamp_; b.pass = pass_;
 }
 
-void BrickCache::read_brick(uint64_t code, void* dst) const {
-    int3 m = vt::min_box(code, cfg_.Lc, cfg_.nLevels);
+void BrickCache::read_brick(uint64_t page, void* dst) const {
+    const int Lc = cfg_.Lc, sh = cfg_.nLevels - cfg_.Lc;
+    const uint64_t msk = (1ull << Lc) - 1;
+    int3 m = make_int3((int)((page >> (2 * Lc)) << sh), (int)(((page >> Lc) & msk) << sh), (int)((page & msk) << sh));
     int s[3] = {m.x - cfg_.inc, m.y - cfg_.inc, m.z - cfg_.inc};
     int e[3] = {s[0] + D_, s[1] + D_, s[2] + D_};
     volume_read_native(cfg_.vol, s, e, dst);

@@ -4,7 +4,8 @@
  *
  * Device tier: a slab of `deviceSlots` bricks of (edge + 2*inc)^3 voxels and
  * a direct-mapped page table indexed by brick Morton code (8^levelCubes
- * entries: slot >= 0, -1 absent, -2 requested this pass).  Kernels look
+ * entries indexed bx << 2Lc | by << Lc | bz: slot >= 0, -1 absent, -2
+ * requested this pass).  Bricks are keyed by that page index throughout.  Kernels look
  * bricks up with one load and request absent ones with one atomicCAS; each
  * use stamps the slot with the pass number, and eviction between passes
  * takes the least recently used slots.

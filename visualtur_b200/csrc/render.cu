@@ -116,14 +116,27 @@ struct Stk {
     unsigned long long e[VT_STACK];
 };
 
+/* stack entry helpers (layout in vt_kernels.h) */
+__device__ __forceinline__ unsigned long long make_entry(unsigned int idx, int level, unsigned int x, unsigned int y,
+                                                         unsigned int z) {
+    return ((unsigned long long)idx << VT_E_INDEX_SHIFT) | ((unsigned long long)level << VT_E_LEVEL_SHIFT) |
+           ((unsigned long long)x << (2 * VT_E_COORD_BITS)) | ((unsigned long long)y << VT_E_COORD_BITS) | z;
+}
+__device__ __forceinline__ int e_level(unsigned long long e) { return (int)((e >> VT_E_LEVEL_SHIFT) & 15u); }
+__device__ __forceinline__ unsigned int e_index(unsigned long long e) { return (unsigned int)(e >> VT_E_INDEX_SHIFT); }
+__device__ __forceinline__ unsigned int e_x(unsigned long long e) { return (unsigned int)(e >> (2 * VT_E_COORD_BITS)) & 0x7FFu; }
+__device__ __forceinline__ unsigned int e_y(unsigned long long e) { return (unsigned int)(e >> VT_E_COORD_BITS) & 0x7FFu; }
+__device__ __forceinline__ unsigned int e_z(unsigned long long e) { return (unsigned int)e & 0x7FFu; }
+
+/* sampler for the brick at brick coordinates (bx,by,bz) */
 template <int VTYPE, bool SLAB>
-__device__ __forceinline__ void setup_sampler(const TraceArgs& A, unsigned long long brick, Samp& s,
-                                              int* slot) {
+__device__ __forceinline__ void setup_sampler(const TraceArgs& A, unsigned int bx, unsigned int by, unsigned int bz,
+                                              unsigned int pidx, Samp& s, int* slot) {
     const DevBricks& B = A.br;
     if (SLAB) {
-        int3 bm = min_box(brick, A.oct.Lc, A.oct.nLevels);
-        s.ox = bm.x - B.inc; s.oy = bm.y - B.inc; s.oz = bm.z - B.inc;
-        int sl = B.page[brick - B.pageBase];
+        const int sh = A.oct.nLevels - A.oct.Lc;
+        s.ox = (int)(bx << sh) - B.inc; s.oy = (int)(by << sh) - B.inc; s.oz = (int)(bz << sh) - B.inc;
+        int sl = B.page[pidx];
         *slot = sl;
         if (sl < 0) return;
         s.base = (const char*)B.slab + (size_t)sl * (size_t)B.brickVol * (VTYPE == 0 ? 4 : 1);
@@ -157,182 +170,177 @@ struct Ray {
 
 enum { RAY_RUNNING = 0, RAY_DONE = 1, RAY_SUSPENDED = 2 };
 
-/* requests brick `brick` once per pass (page -1 -> -2) */
-__device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned long long brick) {
-    int old = atomicCAS(&A.br.page[brick - A.br.pageBase], -1, -2);
+/* requests page `pidx` once per pass (page -1 -> -2) */
+__device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned int pidx) {
+    int old = atomicCAS(&A.br.page[pidx], -1, -2);
     if (old == -1) {
         unsigned int q = atomicAdd(A.ctl.n_req, 1u);
-        if (q < A.ctl.req_cap) A.ctl.req[q] = brick;
+        if (q < A.ctl.req_cap) A.ctl.req[q] = pidx;
         else atomicOr(A.ctl.err, VT_KERR_REQUEST_FULL);
     }
 }
 
-/* Advances one ray's DFS by at most `budget` pops (src/Octree.cu:620-720
- * interleaved with src/rayCaster.cu:139-265).  Returns RAY_DONE when the
- * ray is shaded or exhausted, RAY_SUSPENDED when its next candidate's brick
- * is not resident (the candidate stays on the stack), RAY_RUNNING when the
- * budget ran out. */
+/* Expands the inner node `ent` (_cuda_searchChildrenValidAndHit2,
+ * src/Octree.cu:375-532, with membership from the flattened child mask):
+ * children hit by the ray with tfar >= 0 are sorted by (tnear, tfar)
+ * (src/Octree.cu:665-706) and pushed far to near. */
+__device__ __forceinline__ bool expand(const TraceArgs& A, const RayInv& r, Stk& st, int& top,
+                                       unsigned long long ent, unsigned int* cnt, bool sortChildren) {
+    const DevOctree& O = A.oct;
+    const int nLevels = O.nLevels, Lo = O.Lo;
+    const int level = e_level(ent);
+    const unsigned int px_ = e_x(ent), py_ = e_y(ent), pz_ = e_z(ent);
+    const uint2 nd = O.nodes[e_index(ent)];
+    const int cl = level + 1;
+    const int cd = 1 << (nLevels - cl);
+    const int mx = (int)(px_ << (nLevels - level)), my = (int)(py_ << (nLevels - level)), mz = (int)(pz_ << (nLevels - level));
+    /* the children's faces lie on 3 planes per axis: the slab products of
+     * all 8 children are these 9 values (the same float operations the
+     * reference performs per child, src/Octree.cu:258-330) */
+    const float x0 = ((float)mx - r.o.x) * r.dx, x1 = ((float)(mx + cd) - r.o.x) * r.dx,
+                x2 = ((float)(mx + 2 * cd) - r.o.x) * r.dx;
+    const float y0 = ((float)my - r.o.y) * r.dy, y1 = ((float)(my + cd) - r.o.y) * r.dy,
+                y2 = ((float)(my + 2 * cd) - r.o.y) * r.dy;
+    const float z0 = ((float)mz - r.o.z) * r.dz, z1 = ((float)(mz + cd) - r.o.z) * r.dz,
+                z2 = ((float)(mz + 2 * cd) - r.o.z) * r.dz;
+    const bool sx = r.dx >= 0, sy = r.dy >= 0, sz = r.dz >= 0;
+    const unsigned int m = nd.y;
+    unsigned long long cent[8];
+    float ctn[8], ctf[8];
+    int nv = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if ((m >> k) & 1u) {
+            const int kx = (k >> 2) & 1, ky = (k >> 1) & 1, kz = k & 1;
+            const float xa = kx ? x1 : x0, xb = kx ? x2 : x1;
+            const float ya = ky ? y1 : y0, yb = ky ? y2 : y1;
+            const float za = kz ? z1 : z0, zb = kz ? z2 : z1;
+            float a, b;
+            if (slab_t(sx ? xa : xb, sx ? xb : xa, sy ? ya : yb, sy ? yb : ya, sz ? za : zb, sz ? zb : za, &a, &b) &&
+                b >= 0.0f) {
+                unsigned int cidx = cl < Lo ? nd.x + __popc(m & ((1u << k) - 1u)) : 0u;
+                cent[nv] = make_entry(cidx, cl, (px_ << 1) | kx, (py_ << 1) | ky, (pz_ << 1) | kz);
+                ctn[nv] = a; ctf[nv] = b;
+                nv++;
+            }
+        }
+    }
+    if (sortChildren) {
+        if (nv == 2) {
+            /* one pass of the bubble sort decides two children */
+            if (ctn[0] > ctn[1] || (ctn[0] == ctn[1] && ctf[0] > ctf[1])) {
+                unsigned long long te = cent[0]; cent[0] = cent[1]; cent[1] = te;
+            }
+        } else if (nv > 2) {
+            int n = nv;
+            while (n != 0) {
+                int newn = 0;
+                for (int q = 1; q < nv; q++) {
+                    if (ctn[q - 1] > ctn[q] || (ctn[q - 1] == ctn[q] && ctf[q - 1] > ctf[q])) {
+                        unsigned long long te = cent[q]; cent[q] = cent[q - 1]; cent[q - 1] = te;
+                        float tt = ctn[q]; ctn[q] = ctn[q - 1]; ctn[q - 1] = tt;
+                        tt = ctf[q]; ctf[q] = ctf[q - 1]; ctf[q - 1] = tt;
+                        newn = q;
+                    }
+                }
+                n = newn;
+            }
+        }
+    }
+    if (top + nv >= VT_STACK) {
+        if (sortChildren) atomicOr(A.ctl.err, VT_KERR_STACK);   /* lookahead walks only stop */
+        top = -1;
+        return false;
+    }
+    for (int q = nv - 1; q >= 0; q--) st.e[++top] = cent[q];
+    if ((unsigned int)(top + 1) > cnt[VT_C_MAXSTACK]) cnt[VT_C_MAXSTACK] = top + 1;
+    return true;
+}
+
+/* Advances one ray's DFS by at most `budget` steps (src/Octree.cu:620-720
+ * interleaved with src/rayCaster.cu:139-265): inner nodes are expanded
+ * until a candidate is on top, then the candidate is marched.  Returns
+ * RAY_DONE when the ray is shaded or exhausted, RAY_SUSPENDED when its next
+ * candidate's brick is not resident (the candidate stays on the stack),
+ * RAY_RUNNING when the budget ran out. */
 template <int VTYPE, bool SLAB, int U>
 __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, int budget) {
     const DevOctree& O = A.oct;
-    const int nLevels = O.nLevels, Lo = O.Lo;
-    const int codeBits = 3 * Lo + 1;
-    const unsigned long long codeMask = (1ull << codeBits) - 1ull;
+    const int nLevels = O.nLevels, Lo = O.Lo, Lc = O.Lc;
     const int dimO = 1 << (nLevels - Lo);
-    const int shiftOC = 3 * (Lo - O.Lc);
-    while (R.top >= 0) {
-        if (budget-- == 0) return RAY_RUNNING;
-        unsigned long long ent = st.e[R.top];
-        unsigned long long code = ent & codeMask;
-        unsigned int idx = (unsigned int)(ent >> codeBits);
-        int level = code_level(code);
-        int3 mb = min_box(code, level, nLevels);
-        if (level == Lo) {
-            /* candidate: brick lookup (lruCache::updateCube, src/lruCache.cu:177-291) */
-            unsigned long long brick = code >> shiftOC;
-            Samp s; int slot;
-            setup_sampler<VTYPE, SLAB>(A, brick, s, &slot);
-            if (SLAB && slot < 0) {
-                if (slot == -1) request_brick(A, brick);
-                cnt[VT_C_DEVMISSES]++;
-                return RAY_SUSPENDED;
-            }
+    for (;;) {
+        unsigned long long ent;
+        for (;;) {
+            if (R.top < 0) return RAY_DONE;   /* exhausted: background */
+            ent = st.e[R.top];
+            if (e_level(ent) == Lo) break;
+            if (budget-- == 0) return RAY_RUNNING;
             R.top--;
-            cnt[VT_C_CANDIDATES]++;
-            if (SLAB) { cnt[VT_C_DEVHITS]++; A.br.stamp[slot] = A.br.pass; }
-            if (A.ctl.touched) {
-                unsigned long long tn = (code >> A.ctl.touch_shift) - A.ctl.touch_base;
-                atomicOr(&A.ctl.touched[tn >> 5], 1u << (tn & 31));
-            }
-            float tn, tf;
-            if (!slab(R.r, mb.x, mb.y, mb.z, mb.x + dimO, mb.y + dimO, mb.z + dimO, &tn, &tf)) continue;
-            float3 X;
-            unsigned int ns = 0;
-            bool h = march<VTYPE, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
-            cnt[VT_C_SAMPLES] += ns;
-            if (h) {
-                /* shade (src/rayCaster.cu:238-250) */
-                float3 n = normal_at<VTYPE>(s, X);
-                cnt[VT_C_NSAMPLES] += 6;
-                float3 l = normalize(sub(X, A.light));
-                float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
-                float a = X.y / 256.0f;
-                R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
-                R.hit = true; R.node = code; R.brick = brick; R.n = n;
-                R.t = dot(sub(X, R.r.o), R.dir);
-                return RAY_DONE;
-            }
-            continue;
+            cnt[VT_C_EXPANSIONS]++;
+            if (!expand(A, R.r, st, R.top, ent, cnt, true)) return RAY_DONE;
         }
-        /* expansion: _cuda_searchChildrenValidAndHit2 (src/Octree.cu:375-532)
-         * with membership from the flattened child mask */
+        if (budget-- == 0) return RAY_RUNNING;
+        /* candidate: brick lookup (lruCache::updateCube, src/lruCache.cu:177-291) */
+        const unsigned int x = e_x(ent), y = e_y(ent), z = e_z(ent);
+        const unsigned int bx = x >> (Lo - Lc), by = y >> (Lo - Lc), bz = z >> (Lo - Lc);
+        const unsigned int pidx = (bx << (2 * Lc)) | (by << Lc) | bz;
+        Samp s; int slot;
+        setup_sampler<VTYPE, SLAB>(A, bx, by, bz, pidx, s, &slot);
+        if (SLAB && slot < 0) {
+            if (slot == -1) request_brick(A, pidx);
+            cnt[VT_C_DEVMISSES]++;
+            return RAY_SUSPENDED;
+        }
         R.top--;
-        cnt[VT_C_EXPANSIONS]++;
-        uint2 nd = O.nodes[level][idx];
-        const int cl = level + 1;
-        const int cd = 1 << (nLevels - cl);
-        unsigned long long cent[8];
-        float ctn[8], ctf[8];
-        int nv = 0;
-        unsigned int m = nd.y;
-        /* the children's faces lie on 3 planes per axis: the slab products
-         * of all 8 children are these 9 values (the same float operations
-         * the reference performs per child, src/Octree.cu:258-330) */
-        const float x0 = ((float)mb.x - R.r.o.x) * R.r.dx, x1 = ((float)(mb.x + cd) - R.r.o.x) * R.r.dx,
-                    x2 = ((float)(mb.x + 2 * cd) - R.r.o.x) * R.r.dx;
-        const float y0 = ((float)mb.y - R.r.o.y) * R.r.dy, y1 = ((float)(mb.y + cd) - R.r.o.y) * R.r.dy,
-                    y2 = ((float)(mb.y + 2 * cd) - R.r.o.y) * R.r.dy;
-        const float z0 = ((float)mb.z - R.r.o.z) * R.r.dz, z1 = ((float)(mb.z + cd) - R.r.o.z) * R.r.dz,
-                    z2 = ((float)(mb.z + 2 * cd) - R.r.o.z) * R.r.dz;
-        const bool px = R.r.dx >= 0, py = R.r.dy >= 0, pz = R.r.dz >= 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            if ((m >> k) & 1u) {
-                const int kx = (k >> 2) & 1, ky = (k >> 1) & 1, kz = k & 1;
-                const float xa = kx ? x1 : x0, xb = kx ? x2 : x1;
-                const float ya = ky ? y1 : y0, yb = ky ? y2 : y1;
-                const float za = kz ? z1 : z0, zb = kz ? z2 : z1;
-                float a, b;
-                if (slab_t(px ? xa : xb, px ? xb : xa, py ? ya : yb, py ? yb : ya, pz ? za : zb, pz ? zb : za, &a, &b) &&
-                    b >= 0.0f) {
-                    unsigned long long cidx = nd.x + __popc(m & ((1u << k) - 1u));
-                    cent[nv] = (cidx << codeBits) | ((code << 3) + (unsigned long long)k);
-                    ctn[nv] = a; ctf[nv] = b;
-                    nv++;
-                }
-            }
+        cnt[VT_C_CANDIDATES]++;
+        if (SLAB) { cnt[VT_C_DEVHITS]++; A.br.stamp[slot] = A.br.pass; }
+        if (A.ctl.touched) {
+            const int d = A.ctl.touch_shift / 3;   /* Lo - trace level */
+            unsigned long long tn = (spread3(x >> d) << 2) | (spread3(y >> d) << 1) | spread3(z >> d);
+            atomicOr(&A.ctl.touched[tn >> 5], 1u << (tn & 31));
         }
-        /* bubble sort by (tnear, tfar), src/Octree.cu:665-706 */
-        int n = nv;
-        while (n != 0) {
-            int newn = 0;
-            for (int q = 1; q < nv; q++) {
-                if (ctn[q - 1] > ctn[q] || (ctn[q - 1] == ctn[q] && ctf[q - 1] > ctf[q])) {
-                    unsigned long long te = cent[q]; cent[q] = cent[q - 1]; cent[q - 1] = te;
-                    float tt = ctn[q]; ctn[q] = ctn[q - 1]; ctn[q - 1] = tt;
-                    tt = ctf[q]; ctf[q] = ctf[q - 1]; ctf[q - 1] = tt;
-                    newn = q;
-                }
-            }
-            n = newn;
-        }
-        if (R.top + nv >= VT_STACK) {
-            atomicOr(A.ctl.err, VT_KERR_STACK);
-            R.top = -1;
+        const int mbx = (int)(x << (nLevels - Lo)), mby = (int)(y << (nLevels - Lo)), mbz = (int)(z << (nLevels - Lo));
+        float tn, tf;
+        if (!slab(R.r, mbx, mby, mbz, mbx + dimO, mby + dimO, mbz + dimO, &tn, &tf)) continue;
+        float3 X;
+        unsigned int ns = 0;
+        bool h = march<VTYPE, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
+        cnt[VT_C_SAMPLES] += ns;
+        if (h) {
+            /* shade (src/rayCaster.cu:238-250) */
+            float3 n = normal_at<VTYPE>(s, X);
+            cnt[VT_C_NSAMPLES] += 6;
+            float3 l = normalize(sub(X, A.light));
+            float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
+            float a = X.y / 256.0f;
+            R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
+            R.hit = true; R.node = node_code(x, y, z, Lo); R.brick = node_code(bx, by, bz, Lc); R.n = n;
+            R.t = dot(sub(X, R.r.o), R.dir);
             return RAY_DONE;
         }
-        for (int q = nv - 1; q >= 0; q--) st.e[++R.top] = cent[q];
-        if ((unsigned int)(R.top + 1) > cnt[VT_C_MAXSTACK]) cnt[VT_C_MAXSTACK] = R.top + 1;
     }
-    return RAY_DONE;   /* exhausted: background */
 }
 
 /* Speculative requests: walks a copy of a suspended ray's DFS (without
  * marching) and requests up to `lookahead` further absent bricks. */
 template <int VTYPE>
-__device__ void lookahead_requests(const TraceArgs& A, Ray R, Stk& st) {
+__device__ void lookahead_requests(const TraceArgs& A, Ray R, Stk& st, unsigned int* cnt) {
     const DevOctree& O = A.oct;
-    const int nLevels = O.nLevels, Lo = O.Lo;
-    const int codeBits = 3 * Lo + 1;
-    const unsigned long long codeMask = (1ull << codeBits) - 1ull;
-    const int shiftOC = 3 * (Lo - O.Lc);
+    const int Lo = O.Lo, Lc = O.Lc;
     int want = A.ctl.lookahead, pops = 0;
-    unsigned long long last = 0;
+    unsigned int last = 0xFFFFFFFFu;
     while (R.top >= 0 && want > 0 && pops++ < 256) {
         unsigned long long ent = st.e[R.top--];
-        unsigned long long code = ent & codeMask;
-        unsigned int idx = (unsigned int)(ent >> codeBits);
-        int level = code_level(code);
-        if (level == Lo) {
-            unsigned long long brick = code >> shiftOC;
-            if (brick != last && A.br.page[brick - A.br.pageBase] == -1) { request_brick(A, brick); want--; }
-            last = brick;
+        if (e_level(ent) == Lo) {
+            const unsigned int pidx = ((e_x(ent) >> (Lo - Lc)) << (2 * Lc)) | ((e_y(ent) >> (Lo - Lc)) << Lc) |
+                                      (e_z(ent) >> (Lo - Lc));
+            if (pidx != last && A.br.page[pidx] == -1) { request_brick(A, pidx); want--; }
+            last = pidx;
             continue;
         }
-        int3 mb = min_box(code, level, nLevels);
-        uint2 nd = O.nodes[level][idx];
-        const int cd = 1 << (nLevels - level - 1);
-        unsigned long long cent[8];
-        float ctn[8];
-        int nv = 0;
-        for (int k = 0; k < 8; k++) {
-            if ((nd.y >> k) & 1u) {
-                int bx = mb.x + ((k >> 2) & 1) * cd, by = mb.y + ((k >> 1) & 1) * cd, bz = mb.z + (k & 1) * cd;
-                float a, b;
-                if (slab(R.r, bx, by, bz, bx + cd, by + cd, bz + cd, &a, &b) && b >= 0.0f) {
-                    cent[nv] = ((unsigned long long)(nd.x + __popc(nd.y & ((1u << k) - 1u))) << codeBits) |
-                               ((code << 3) + (unsigned long long)k);
-                    ctn[nv++] = a;
-                }
-            }
-        }
-        for (int q = 1; q < nv; q++)      /* near first (order only affects which bricks get asked) */
-            for (int p = q; p > 0 && ctn[p - 1] > ctn[p]; p--) {
-                float tt = ctn[p]; ctn[p] = ctn[p - 1]; ctn[p - 1] = tt;
-                unsigned long long te = cent[p]; cent[p] = cent[p - 1]; cent[p - 1] = te;
-            }
-        if (R.top + nv >= VT_STACK) break;
-        for (int q = nv - 1; q >= 0; q--) st.e[++R.top] = cent[q];
+        unsigned int scratch[VT_C_COUNT];
+        scratch[VT_C_MAXSTACK] = cnt[VT_C_MAXSTACK];
+        if (!expand(A, R.r, st, R.top, ent, scratch, false)) break;   /* order only affects which bricks get asked */
     }
 }
 
@@ -380,7 +388,7 @@ __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, 
     const int N = 1 << A.oct.nLevels;
     float tn, tf;
     /* root test (src/Octree.cu:729) */
-    if (A.oct.rootValid && slab(R.r, 0, 0, 0, N, N, N, &tn, &tf)) { R.top = 0; st.e[0] = 1ull; return RAY_RUNNING; }
+    if (A.oct.rootValid && slab(R.r, 0, 0, 0, N, N, N, &tn, &tf)) { R.top = 0; st.e[0] = make_entry(0, 0, 0, 0, 0); return RAY_RUNNING; }
     return RAY_DONE;   /* background */
 }
 
@@ -418,7 +426,7 @@ __device__ __forceinline__ void suspend_ray(const TraceArgs& A, Ray& R, Stk& st,
         rec.depth = 0; rec.off = 0;   /* pool full: the ray restarts from the root (same result) */
     }
     A.ctl.out[q] = rec;
-    if (SLAB && A.ctl.lookahead > 0) lookahead_requests<VTYPE>(A, R, st);
+    if (SLAB && A.ctl.lookahead > 0) lookahead_requests<VTYPE>(A, R, st, cnt);
 }
 
 __device__ __forceinline__ void flush_counters(const TraceArgs& A, unsigned int* cnt) {

@@ -19,6 +19,7 @@
 #include "vt_kernels.h"
 #include "vt_runtime.h"
 #include "cache.h"
+#include "vt_math.cuh"
 
 using namespace vtrt;
 
@@ -157,7 +158,8 @@ struct vt_handle {
     float fovH = 0, fovW = 0;
     int nLevels = 0, Lo = 0, Lc = 0, inc = 3, edge = 0, D = 0;
     /* flattened octree */
-    std::vector<uint2*> d_nodes;
+    uint2* d_nodes = nullptr;
+    size_t nodeCount = 0;
     int rootValid = 0;
     std::vector<uint64_t> leafBricks;   /* bricks holding reachable candidate nodes */
     /* dense residency */
@@ -224,39 +226,43 @@ static vt_status ensure_suspend_buffers(vt_handle* h, unsigned int rays) {
 
 /* Octree flattening: keeps the nodes reachable from the root through the
  * reference's traversal (src/Octree.cu:620-739) and records, per node, the
- * children its range search accepts -- a property of the node alone. */
+ * children its range search accepts -- a property of the node alone.  All
+ * levels 0..Lo-1 go into one array; a record holds the array index of its
+ * node's first child. */
 static vt_status flatten_octree(vt_handle* h) {
     const vt_octree* o = h->oct;
     const int Lo = h->Lo;
+    if (Lo > VT_MAX_OCTREE_LEVEL) return fail(VT_ERR_UNSUPPORTED, "octreeLevel %d > %d", Lo, VT_MAX_OCTREE_LEVEL);
     const std::vector<uint64_t>& l0 = o->levels[0];
     h->rootValid = (l0.size() >= 2 && (l0[0] == 1 || l0[1] == 1 || (l0[0] < 1 && l0[1] > 1))) ? 1 : 0;
     std::vector<uint64_t> codes(1, 1ull), next;
-    h->d_nodes.assign(Lo, nullptr);
-    const int codeBits = 3 * Lo + 1;
+    std::vector<uint2> all;
     for (int l = 0; l < Lo; l++) {
         const std::vector<uint64_t>& e = o->levels[l + 1];
-        std::vector<uint2> rec(codes.size());
         std::vector<int> mask(codes.size());
 #pragma omp parallel for schedule(dynamic, 4096)
         for (long long i = 0; i < (long long)codes.size(); i++)
             mask[i] = children_mask(e.data(), (int)e.size(), codes[i]);
+        const uint64_t nextBase = all.size() + codes.size();   /* level l+1 starts after level l */
         next.clear();
-        uint64_t base = 0;
+        uint64_t run = 0;
         for (size_t i = 0; i < codes.size(); i++) {
-            rec[i].x = (unsigned int)base;
-            rec[i].y = (unsigned int)mask[i];
+            uint2 r;
+            r.x = (unsigned int)(nextBase + run);
+            r.y = (unsigned int)mask[i];
+            all.push_back(r);
             for (int k = 0; k < 8; k++)
                 if ((mask[i] >> k) & 1) next.push_back((codes[i] << 3) + (uint64_t)k);
-            base += __builtin_popcount(mask[i]);
+            run += __builtin_popcount(mask[i]);
         }
-        if (l + 1 < Lo && next.size() >= (1ull << (64 - codeBits)))
-            return fail(VT_ERR_UNSUPPORTED, "level %d has %zu nodes, more than the stack entry encodes", l + 1, next.size());
-        if (next.size() > 0xFFFFFFFFull) return fail(VT_ERR_UNSUPPORTED, "level %d too large", l + 1);
-        CK(cudaMalloc(&h->d_nodes[l], std::max<size_t>(rec.size(), 1) * sizeof(uint2)));
-        CK(cudaMemcpy(h->d_nodes[l], rec.data(), rec.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+        if (l + 1 < Lo && all.size() + next.size() > VT_MAX_INNER_NODES)
+            return fail(VT_ERR_UNSUPPORTED, "octree has more than %u inner nodes", VT_MAX_INNER_NODES);
         codes.swap(next);
     }
-    /* bricks that hold reachable candidates */
+    h->nodeCount = all.size();
+    CK(cudaMalloc(&h->d_nodes, std::max<size_t>(all.size(), 1) * sizeof(uint2)));
+    CK(cudaMemcpy(h->d_nodes, all.data(), all.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    /* bricks that hold reachable candidates, as Morton codes at levelCubes */
     const int shift = 3 * (Lo - h->Lc);
     h->leafBricks.clear();
     for (size_t i = 0; i < codes.size(); i++) {
@@ -264,6 +270,21 @@ static vt_status flatten_octree(vt_handle* h) {
         if (h->leafBricks.empty() || h->leafBricks.back() != b) h->leafBricks.push_back(b);
     }
     return VT_OK;
+}
+
+/* brick Morton code at levelCubes <-> page-table index (bx << 2Lc | by << Lc | bz) */
+static inline uint64_t code_to_page(uint64_t code, int Lc) {
+    int3 c = vt::min_box(code, Lc, Lc);
+    return ((uint64_t)c.x << (2 * Lc)) | ((uint64_t)c.y << Lc) | (uint64_t)c.z;
+}
+static inline uint64_t page_to_code(uint64_t p, int Lc) {
+    uint64_t m = (1ull << Lc) - 1;
+    return vt::node_code((uint32_t)(p >> (2 * Lc)), (uint32_t)((p >> Lc) & m), (uint32_t)(p & m), Lc);
+}
+static std::vector<uint64_t> to_pages(const std::vector<uint64_t>& codes, int Lc) {
+    std::vector<uint64_t> p(codes.size());
+    for (size_t i = 0; i < codes.size(); i++) p[i] = code_to_page(codes[i], Lc);
+    return p;
 }
 
 static vt_status upload_dense(vt_handle* h) {
@@ -362,7 +383,7 @@ static vt_status init_handle(vt_handle* h) {
         h->cache = new vtrt::BrickCache();
         if ((s = h->cache->init(cc)) != VT_OK) return s;
         if (h->opt.preload && (size_t)p.maxElementsCache >= h->leafBricks.size()) {
-            if ((s = h->cache->preload(h->leafBricks)) != VT_OK) return s;
+            if ((s = h->cache->preload(to_pages(h->leafBricks, h->Lc))) != VT_OK) return s;
         }
         h->req_cap = (unsigned int)std::max<size_t>(h->leafBricks.size(), 1);
         CK(cudaMalloc(&h->d_req, (size_t)h->req_cap * 8));
@@ -409,7 +430,7 @@ extern "C" void vt_destroy(vt_handle* h) {
     if (h->s_int) cudaStreamSynchronize(h->s_int);
     cudaDeviceSynchronize();
     free_ray_buffers(h);
-    for (uint2* p : h->d_nodes) cudaFree(p);
+    cudaFree(h->d_nodes);
     for (int i = 0; i < 2; i++) { cudaFree(h->d_susp[i]); cudaFree(h->d_pool[i]); }
     cudaFree(h->d_vol); cudaFree(h->d_ctl); cudaFree(h->d_views); cudaFree(h->d_req); cudaFree(h->d_touched);
     if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -472,7 +493,8 @@ extern "C" vt_status vt_change_cache(vt_handle* h, int nE, const int cDim[3], in
     cc.deviceSlots = nE; cc.hostSlots = h->p.maxElementsCache_CPU; cc.hostThreads = h->opt.host_threads;
     h->cache = new vtrt::BrickCache();
     if ((s = h->cache->init(cc)) != VT_OK) return s;
-    if (h->opt.preload && (size_t)nE >= h->leafBricks.size() && (s = h->cache->preload(h->leafBricks)) != VT_OK) return s;
+    if (h->opt.preload && (size_t)nE >= h->leafBricks.size() &&
+        (s = h->cache->preload(to_pages(h->leafBricks, h->Lc))) != VT_OK) return s;
     h->lastValid = false;
     return VT_OK;
 }
@@ -482,7 +504,7 @@ static void fill_args(vt_handle* h, TraceArgs& a, int nViews, unsigned int total
     memset(&a, 0, sizeof(a));
     a.views.v = h->d_views; a.views.n = nViews; a.views.totalRays = totalRays;
     a.oct.nLevels = h->nLevels; a.oct.Lo = h->Lo; a.oct.Lc = h->Lc; a.oct.rootValid = h->rootValid;
-    for (int l = 0; l < h->Lo; l++) a.oct.nodes[l] = h->d_nodes[l];
+    a.oct.nodes = h->d_nodes;
     a.br.vtype = h->vol->vtype; a.br.inc = h->inc;
     if (h->opt.resident) {
         a.br.vol = h->d_vol; a.br.P = h->P; a.br.ve = (int)h->ve;
@@ -732,7 +754,7 @@ extern "C" vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n
     b.reserve((size_t)n);
     for (int64_t i = 0; i < n; i++) {
         if (bricks[i] < lo || bricks[i] >= hi) return fail(VT_ERR_INVALID, "brick code %llu not at levelCubes", (unsigned long long)bricks[i]);
-        b.push_back(bricks[i]);
+        b.push_back(code_to_page(bricks[i], h->Lc));
     }
     int64_t got = 0;
     vt_status s = h->cache->prefetch(b, stream ? (cudaStream_t)stream : h->s_int, &got);
@@ -771,7 +793,7 @@ extern "C" vt_status vt_prefetch_hint(vt_handle* h, const uint64_t* bricks, int6
     h->hint.clear();
     for (int64_t i = 0; i < n; i++) {
         if (bricks[i] < lo || bricks[i] >= hi) return fail(VT_ERR_INVALID, "brick code %llu not at levelCubes", (unsigned long long)bricks[i]);
-        h->hint.push_back(bricks[i]);
+        h->hint.push_back(code_to_page(bricks[i], h->Lc));
     }
     return VT_OK;
 }

@@ -27,17 +27,27 @@ struct DevCamera {
     int W, H;
 };
 
-/* Flattened octree: node records of levels 0..Lo-1.  node.x = index of the
- * first child in the next level's array, node.y = 8-bit child mask (bit k =
- * child (code<<3)+k accepted by the reference's range search). */
+/* Flattened octree: records of the reachable nodes of levels 0..Lo-1 in
+ * one array, level after level.  node.x = array index of the first child,
+ * node.y = 8-bit child mask (bit k = child (code<<3)+k accepted by the
+ * reference's range search); children of a node are contiguous. */
 struct DevOctree {
     int nLevels, Lo, Lc, rootValid;
-    const uint2* nodes[VT_MAX_LEVELS];
+    const uint2* nodes;
 };
+
+/* DFS stack entry (8 bytes): node array index, level, and the node's
+ * coordinates in units of its own size (each < 2^level). */
+#define VT_E_COORD_BITS 11
+#define VT_E_LEVEL_SHIFT 33
+#define VT_E_INDEX_SHIFT 37
+#define VT_MAX_OCTREE_LEVEL 11                 /* coordinates fit 11 bits */
+#define VT_MAX_INNER_NODES (1u << 27)          /* index field */
 
 /* Brick storage.  Dense: the whole zero-padded volume, P voxels of zeros on
  * every side; index ((x+P)*ey + (y+P))*ez + (z+P).  Slab: bricks of D^3
- * voxels (edge + 2*inc) in slots; page[code - pageBase] = slot or < 0. */
+ * voxels (edge + 2*inc) in slots; page[(bx << 2Lc) | (by << Lc) | bz] =
+ * slot or < 0, (bx,by,bz) the brick's coordinates in bricks. */
 struct DevBricks {
     const void* vol;  long long vsx, vsy; int P; int ve;   /* ve: padded edge */
     int* page; unsigned long long pageBase; const void* slab; int D; long long brickVol;

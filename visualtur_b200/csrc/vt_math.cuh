@@ -94,6 +94,24 @@ VT_HD uint32_t compact3(uint64_t v) {
     v = (v ^ (v >> 32)) & 0x00000000001FFFFFull;
     return (uint32_t)v;
 }
+/* 3-way bit dilation (dilateInteger, inc/mortonCodeUtil.hpp:31-40): bit k
+ * of v -> bit 3k, for 21-bit v. */
+VT_HD uint64_t spread3(uint32_t v) {
+    uint64_t x = v & 0x1FFFFFu;
+    x = (x | (x << 32)) & 0x001F00000000FFFFull;
+    x = (x | (x << 16)) & 0x001F0000FF0000FFull;
+    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+/* coordinateToIndex (inc/mortonCodeUtil.hpp:146-169) from node coordinates
+ * at `level` (each in [0, 2^level)): sentinel bit 3*level, x in bit 2 of
+ * each triplet. */
+VT_HD uint64_t node_code(uint32_t x, uint32_t y, uint32_t z, int level) {
+    return (1ull << (3 * level)) | (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
+}
+
 /* getMinBoxIndex2 (inc/mortonCodeUtil.hpp:120-144): min corner of node
  * `code` at `level` of an nLevels tree (x in bit 2 of each triplet). */
 VT_HD int3 min_box(uint64_t code, int level, int nLevels) {
