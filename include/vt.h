@@ -281,6 +281,18 @@ vt_status vt_mlp_gradients(vt_mlp* m, const float* dev_x, const float* dev_y, in
 /* FP32 master weights, layer by layer: W (in x out, row-major) then b */
 vt_status vt_mlp_get_weights(vt_mlp* m, float* host, int64_t* n);
 vt_status vt_mlp_set_weights(vt_mlp* m, const float* host, int64_t n);
+/* vt_mlp_forward without any allocation (no counterpart in the reference).
+ * For callers that cannot allocate GPU memory where they run inference --
+ * a render loop in a host that owns the device's memory budget, or a frame
+ * thread that must not call cudaMalloc (it synchronises the device).  The
+ * hidden activations use a fixed 1 MiB device array built into libvt.so,
+ * so batch * (h1 + h2) must be at most 262144 floats (e.g. batch 256 for
+ * 512 + 512 hidden units); larger batches return VT_ERR_INVALID.  The first
+ * call on each device looks the array's address up (cudaGetSymbolAddress):
+ * make that first call before any stream capture.  All calls on a device
+ * share the array: calls that overlap on the GPU (other streams, threads)
+ * race and must be serialised by the caller. */
+vt_status vt_mlp_forward_noalloc(vt_mlp* m, const float* dev_x, int batch, float* dev_p, void* stream);
 
 #ifdef __cplusplus
 }

@@ -129,6 +129,7 @@ _PROTOS = {
     "vt_mlp_gradients": (C.c_int, [_P, _P, _P, C.c_int, _P, C.POINTER(C.c_float)]),
     "vt_mlp_get_weights": (C.c_int, [_P, _P, C.POINTER(C.c_int64)]),
     "vt_mlp_set_weights": (C.c_int, [_P, _P, C.c_int64]),
+    "vt_mlp_forward_noalloc": (C.c_int, [_P, _P, C.c_int, _P, _P]),
 }
 
 _lib = None
@@ -515,6 +516,11 @@ class MLP:
 
     def forward(self, dev_x, batch, dev_p, stream=None):
         check(lib().vt_mlp_forward(self._h, _ptr(dev_x), batch, _ptr(dev_p), stream))
+
+    def forward_noalloc(self, dev_x, batch, dev_p, stream=None):
+        """Same result as forward(); allocates nothing (fixed 1 MiB device
+        scratch, batch * (h1 + h2) <= 262144; calls must not overlap)."""
+        check(lib().vt_mlp_forward_noalloc(self._h, _ptr(dev_x), batch, _ptr(dev_p), stream))
 
     def train_step(self, dev_x, dev_y, batch, lr, stream=None, want_loss=True):
         loss = C.c_float()

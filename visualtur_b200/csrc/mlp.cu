@@ -349,3 +349,61 @@ extern "C" vt_status vt_mlp_set_weights(vt_mlp* m, const float* host, int64_t n)
     CKM(cudaDeviceSynchronize());
     return VT_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Allocation-free inference                                                */
+/* ------------------------------------------------------------------------ */
+/* Some callers cannot allocate GPU memory at the point where they run the
+ * prefetch network: a render loop inside a host application that owns the
+ * device's memory (its own pool, a fixed budget), or a frame thread that
+ * must not call cudaMalloc because it synchronises the device and can stall
+ * the frame.  vt_mlp_forward_noalloc serves them: its two hidden-layer
+ * activations live in this fixed, file-scope device array instead of the
+ * handle's lazily allocated buffers.  Every GPU that loads libvt.so holds
+ * the array (1 MiB) until the process exits. */
+#define VT_MLP_NOALLOC_FLOATS (1 << 18)
+static __device__ __align__(256) float g_mlp_noalloc_scratch[VT_MLP_NOALLOC_FLOATS];
+
+#include <mutex>
+static std::mutex g_noalloc_mu;
+static float* g_noalloc_dev[256];   /* per device: address of the array, looked up once */
+
+extern "C" vt_status vt_mlp_forward_noalloc(vt_mlp* m, const float* dev_x, int batch, float* dev_p, void* stream) {
+    vtrt::clear_error();
+    if (!m || !dev_x || !dev_p || batch <= 0) return vtrt::fail(VT_ERR_INVALID, "vt_mlp_forward_noalloc: bad arguments");
+    const int* d = m->dims;
+    long long need = (long long)batch * (d[1] + d[2]);
+    if (need > VT_MLP_NOALLOC_FLOATS)
+        return vtrt::fail(VT_ERR_INVALID,
+                          "vt_mlp_forward_noalloc: batch %d x (%d + %d) hidden units = %lld floats exceeds the "
+                          "static scratch of %d floats", batch, d[1], d[2], need, VT_MLP_NOALLOC_FLOATS);
+    int dev = 0;
+    CKM(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return vtrt::fail(VT_ERR_UNSUPPORTED, "device ordinal %d", dev);
+    float* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_dev[dev]) {
+            /* host code only sees a stand-in for the array: its device address
+             * comes from the runtime, once per device, with that device current */
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_mlp_noalloc_scratch);
+            if (e != cudaSuccess)
+                return vtrt::fail(VT_ERR_CUDA, "cudaGetSymbolAddress(g_mlp_noalloc_scratch): %s", cudaGetErrorString(e));
+            g_noalloc_dev[dev] = (float*)p;
+        }
+        scratch = g_noalloc_dev[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    float* h1 = scratch;
+    float* h2 = scratch + (size_t)batch * d[1];
+    /* every activation element is written before it is read, so the array's
+     * leftovers from the previous call need no clearing */
+    CKM((gemm<float, __nv_bfloat16>(dev_x, d[0], 1, m->wb[0], d[1], 1, h1, d[1], batch, d[1], d[0], m->b[0],
+                                    ACT_RELU, 0, s)));
+    CKM((gemm<float, __nv_bfloat16>(h1, d[1], 1, m->wb[1], d[2], 1, h2, d[2], batch, d[2], d[1], m->b[1],
+                                    ACT_RELU, 0, s)));
+    CKM((gemm<float, __nv_bfloat16>(h2, d[2], 1, m->wb[2], d[3], 1, dev_p, d[3], batch, d[3], d[2], m->b[2],
+                                    ACT_SIGMOID, 0, s)));
+    return VT_OK;
+}
