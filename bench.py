@@ -275,7 +275,9 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, frame=0):
 # ----------------------------------------------------------------------------- arms
 class Launcher:
     """Renders consecutive orbit frames in launches of `batch` views; with a
-    predictor, hands the renderer the predicted bricks of the next launch."""
+    predictor, hands the renderer the predicted bricks of this launch and the
+    next one: their host-tier reads overlap this launch's first pass, and
+    those still absent after its last pass are filled for the next launch."""
 
     def __init__(self, wl, r, cfg, torch, dev, stream, batch=1, predictor=None, threshold=0.25, warm=False):
         self.wl, self.r, self.cfg, self.torch, self.stream = wl, r, cfg, torch, stream
@@ -297,7 +299,7 @@ class Launcher:
         self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
 
     def launch(self, cams, next_cams=()):
-        self.hint(list(next_cams))
+        self.hint(list(cams) + list(next_cams))
         sp = self.stream.cuda_stream
         if self.batch == 1:
             self.r.set_camera(cams[0])
@@ -455,7 +457,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
                         "trace_ms_per_step": round(trace_tot / args.steps, 4),
                         "device_hit_rate": round(st["device_hits"] / max(1, st["device_hits"] + st["device_misses"]), 5),
                         "bricks_requested": st["bricks_requested"], "bricks_loaded": st["bricks_loaded_disk"],
-                        "bricks_prefetched": st["bricks_prefetched"],
+                        "bricks_prefetched": st["bricks_prefetched"], "bricks_hinted": st["bricks_hinted"],
+                        "bricks_staged": st["bricks_staged"],
                         "hits": st["hits"], "samples": st["samples"], "candidates": st["candidates"],
                         "expansions": st["expansions"]},
     }

@@ -169,6 +169,10 @@ typedef struct {
     int pops;              /* persistent: traversal steps between warp refills */
     int preload;           /* 1: load every needed brick at create when they fit */
     int use_graph;         /* 1: pass 0 of a frame replays a captured CUDA graph */
+    int refine;            /* isovalue crossing refinement: 0 = one linear step, as the
+                              reference (src/rayCaster.cu:227-228); k in 1..16 = k
+                              bisection steps on the bracketing samples, then the
+                              linear step.  Node and brick ids do not depend on it. */
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -247,6 +251,8 @@ typedef struct {
     int64_t device_hits, device_misses, host_hits, host_misses;
     int64_t max_stack;
     int64_t launches;               /* libvt kernels launched (cumulative) */
+    int64_t bricks_hinted;          /* bricks named by vt_prefetch and by hints a frame consumed */
+    int64_t bricks_staged;          /* of those, absent from the device cache when staged */
     double  ms_last_frame, ms_stall_last_frame, bytes_h2d_last_frame;
     double  ms_trace_last_frame;    /* device time of the trace kernels of the last frame */
     double  ms_prefetch_last_frame; /* host time of the hinted prefetch's device fill */

@@ -36,7 +36,7 @@ class orc_camera(C.Structure):
 class orc_render_params(C.Structure):
     _fields_ = [("levelO", C.c_int), ("levelC", C.c_int), ("cubeInc", C.c_int), ("iso", C.c_float),
                 ("light", orc_f3), ("nthreads", C.c_int), ("ray_begin", C.c_int), ("ray_end", C.c_int),
-                ("ray_stride", C.c_int), ("dirs", C.c_void_p)]
+                ("ray_stride", C.c_int), ("dirs", C.c_void_p), ("refine", C.c_int)]
 
 
 class orc_render_out(C.Structure):
@@ -172,7 +172,7 @@ class Octree:
 
 
 def render(octree, volume, cam, levelO, levelC, cubeInc=3, iso=None, light=(0.0, 512.0, 0.0), nthreads=0,
-           ray_begin=0, ray_end=0, ray_stride=1, dirs=None):
+           ray_begin=0, ray_end=0, ray_stride=1, dirs=None, refine=0):
     """Renders one frame; returns per-ray arrays and aggregate counters."""
     vol = np.ascontiguousarray(volume)
     vtype = 1 if vol.dtype == np.uint8 else 0
@@ -188,6 +188,7 @@ def render(octree, volume, cam, levelO, levelC, cubeInc=3, iso=None, light=(0.0,
     p.iso = octree.iso if iso is None else iso
     p.light = orc_f3(*light)
     p.nthreads, p.ray_begin, p.ray_end, p.ray_stride = nthreads, ray_begin, ray_end, ray_stride
+    p.refine = refine
     d = None
     if dirs is not None:
         d = np.ascontiguousarray(dirs, np.float32)

@@ -245,10 +245,17 @@ static inline V3 normal_at(V3 p, const B& d, I3 mb) {
 }
 
 /* The march loop shared by cuda_rayCaster (:166-237) and
- * cuda_rayCasterCube (:285-328); TSteps is int or float. */
+ * cuda_rayCasterCube (:285-328); TSteps is int or float.
+ *
+ * refine > 0 is the renderer's bisection mode (an extension: the
+ * reference's own refinement loop at :214-226 is compiled out): before the
+ * linear step, the pair (previous sample, crossing sample) is halved
+ * `refine` times; a midpoint whose iso - value is strictly on the same side
+ * as the previous sample's replaces the previous sample, otherwise it
+ * replaces the crossing sample.  Every midpoint counts as a sample. */
 template <class B, class TSteps>
 static inline bool march(V3 origin, V3 ray, float tnear, TSteps maxStep, const B& data, I3 minBox,
-                         float iso, V3* Xhit, int64_t* nsamp) {
+                         float iso, V3* Xhit, int64_t* nsamp, int refine = 0) {
     bool hit = false;
     V3 Xnear = origin + tnear * ray;
     V3 Xfar = Xnear, Xnew = Xnear;
@@ -268,8 +275,17 @@ static inline bool march(V3 origin, V3 ray, float tnear, TSteps maxStep, const B
                 ant = sig;
                 Xfar = Xnear;
             } else {
+                V3 lo = Xfar, hi = Xnear;
+                for (int k = 0; k < refine; k++) {
+                    V3 mid = (lo + hi) * 0.5f;
+                    float vm = interp(mid, data, minBox); (*nsamp)++;
+                    bool same = (((iso - ant) < 0.0) && ((iso - vm) < 0.0)) ||
+                                (((iso - ant) > 0.0) && ((iso - vm) > 0.0));
+                    if (same) { lo = mid; ant = vm; }
+                    else { hi = mid; sig = vm; }
+                }
                 float a = (iso - ant) / (sig - ant);
-                Xnew = Xfar * (1.0f - a) + Xnear * a;
+                Xnew = lo * (1.0f - a) + hi * a;
                 hit = true;
                 steps = maxStep;
             }
@@ -544,7 +560,7 @@ extern "C" int orc_render_frame(const orc_octree* o, const void* vol, int vtype,
                 Brick B = {&V, minBox, D, &oob};
                 int maxStep = d2i(ceil((tf - tn) / 0.5));
                 V3 Xh;
-                if (march(origin, ray, tn, maxStep, B, minBox, p->iso, &Xh, &samp)) {
+                if (march(origin, ray, tn, maxStep, B, minBox, p->iso, &Xh, &samp, p->refine)) {
                     hit = true; hitNode = cid; hitBrick = cubeID; X = Xh;
                     n = normal_at(X, B, minBox);
                     nsamp += 6;

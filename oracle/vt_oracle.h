@@ -81,6 +81,7 @@ typedef struct {
     int nthreads;        /* 0 = OpenMP default */
     int ray_begin, ray_end, ray_stride;   /* subset of ray ids; end<=0 -> all */
     const orc_f3* dirs;  /* optional per-ray directions (NULL: cuda_updateRays) */
+    int refine;          /* 0: reference refinement; k: k bisection steps first */
 } orc_render_params;
 
 typedef struct {

@@ -23,7 +23,7 @@ N_TOL = 1e-3        # radians
 RGB8_TOL = 1        # LSB
 
 
-def product_render(case, workdir, mode, vol=None, extra_ops=()):
+def product_render(case, workdir, mode, vol=None, extra_ops=(), refine=0):
     c = F.CASES[case]
     vol = F.case_volume(case) if vol is None else vol
     fm = vt.FileManager.wrap(vol)
@@ -35,7 +35,7 @@ def product_render(case, workdir, mode, vol=None, extra_ops=()):
     opt = vt.default_options(resident=1 if mode in ("resident", "persist") else 0, record_hits=1,
                              persistent=1 if mode in ("persist", "demand_la") else 0,
                              lookahead=3 if mode == "demand_la" else 0, pops=3,
-                             unroll={"persist": 4, "demand_la": 2, "slab": 8}.get(mode, 1))
+                             unroll={"persist": 4, "demand_la": 2, "slab": 8}.get(mode, 1), refine=refine)
     p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=c["levelO"],
                        levelCubes=c["levelC"], dimCube=1 << (int(np.log2(c["n"])) - c["levelC"]),
                        cubeInc=c["inc"], distance=c["dist"], fov_H=c["fov"], fov_W=c["fov"],
@@ -52,13 +52,13 @@ def product_render(case, workdir, mode, vol=None, extra_ops=()):
     return dict(rgba=rgba, rgb8=rgb8, node=node, brick=brick, t=t, normal=nrm, stats=st)
 
 
-def oracle_render(case, workdir, vol=None, extra_ops=()):
+def oracle_render(case, workdir, vol=None, extra_ops=(), refine=0):
     c = F.CASES[case]
     vol = F.case_volume(case) if vol is None else vol
     o = orc.Octree(F.case_octree(case, workdir))
     cam = F.oracle_camera(case)
     orc.apply_ops(cam, extra_ops)
-    return orc.render(o, vol, cam, c["levelO"], c["levelC"], c["inc"])
+    return orc.render(o, vol, cam, c["levelO"], c["levelC"], c["inc"], refine=refine)
 
 
 def assert_parity(a, b):
@@ -85,6 +85,22 @@ def test_render_parity(case, mode, workdir, cuda):
     assert a["stats"]["candidates"] == b["agg"]["candidates"]
     if mode.startswith("demand"):
         assert a["stats"]["passes"] > 1 and a["stats"]["bricks_requested"] > 24
+
+
+@pytest.mark.parametrize("mode", ["resident", "demand_la"])
+@pytest.mark.parametrize("case", ["c1", "s64rot"])
+def test_bisection_mode_parity(case, mode, workdir, cuda):
+    """Bisection refinement (5 steps) against the oracle in the same mode;
+    node and brick ids equal those of the reference refinement."""
+    a = product_render(case, workdir, mode, refine=5)
+    b = oracle_render(case, workdir, refine=5)
+    assert_parity(a, b)
+    assert a["stats"]["samples"] == b["agg"]["samples"]
+    base = oracle_render(case, workdir)
+    assert np.array_equal(a["node"], base["node"]) and np.array_equal(a["brick"], base["brick"])
+    hit = base["node"] != 0
+    assert b["agg"]["samples"] == base["agg"]["samples"] + 5 * int(hit.sum())
+    assert not np.array_equal(a["t"][hit], base["t"][hit])
 
 
 def test_camera_rays_bitwise(cuda, workdir):

@@ -2,10 +2,14 @@
 
 Traces of marched coarse nodes are logged by the renderer on random
 fly-throughs, the network is trained on the GPU by libvt's kernels, and a
-held-out spline fly-through is rendered with demand paging alone and with
-the network's prefetch hints.  The images must be identical frame by frame
-(a prediction never changes a pixel) and the learned hints must raise the
-device-cache hit rate and cut the demand passes."""
+held-out spline fly-through is rendered from a cold cache with demand
+paging alone and with the network's prefetch hints.  The images must be
+identical frame by frame (a prediction never changes a pixel); the hints
+must load bricks ahead of demand, raise the device-cache hit rate and cut
+the demand requests and passes.  The device cache holds every brick of the
+scene: each frame of this small scene touches most of its bricks, so a
+smaller cache is refilled within every frame and leaves no slot that the
+next frame's prefetch may take."""
 import numpy as np
 import pytest
 
@@ -57,10 +61,10 @@ def test_learned_prefetch_gains_over_demand_paging(scene, cuda):
     hist = P.train(torch, X, Y, epochs=40, batch=128, lr=2e-3)
     assert hist[-1] < 0.6 * hist[0]
 
-    # held-out spline; device cache holds a quarter of the bricks
+    # held-out spline, cold start
     pos, tgt = pf.random_flythrough(np.random.default_rng(999), N, 60, 1.3 * N, 1.7 * N)
     cams = [pf.look_at(W, H, 50.0, FOV, p_, t_) for p_, t_ in zip(pos, tgt)]
-    dev = max(64, len(bricks) // 4)
+    dev = len(bricks)
     results = {}
     for mode in ("demand", "learned"):
         r, keep2 = make(vol, path, dev, len(bricks), resident=0, preload=0, record_hits=0)
@@ -81,5 +85,8 @@ def test_learned_prefetch_gains_over_demand_paging(scene, cuda):
         r.close()
     for a, b in zip(results["demand"]["imgs"], results["learned"]["imgs"]):
         assert np.array_equal(a, b)
-    assert results["learned"]["hit_rate"] > results["demand"]["hit_rate"]
-    assert results["learned"]["passes"] < results["demand"]["passes"]
+    dem, lrn = results["demand"], results["learned"]
+    assert lrn["stats"]["bricks_prefetched"] > 0
+    assert lrn["hit_rate"] > dem["hit_rate"]
+    assert lrn["stats"]["bricks_requested"] < dem["stats"]["bricks_requested"]
+    assert lrn["passes"] < dem["passes"]

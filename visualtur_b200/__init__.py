@@ -46,14 +46,15 @@ class vt_params(C.Structure):
 class vt_options(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("resident", "tile_w", "tile_h", "unroll", "lookahead", "max_passes",
                                          "host_threads", "record_trace", "trace_level", "record_hits",
-                                         "persistent", "blocks_per_sm", "pops", "preload", "use_graph")]
+                                         "persistent", "blocks_per_sm", "pops", "preload", "use_graph", "refine")]
 
 
 class vt_stats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "frames", "rays", "hits", "samples", "normal_samples", "candidates", "expansions", "passes",
         "bricks_requested", "bricks_loaded_host", "bricks_loaded_disk", "bricks_prefetched",
-        "device_hits", "device_misses", "host_hits", "host_misses", "max_stack", "launches")] + \
+        "device_hits", "device_misses", "host_hits", "host_misses", "max_stack", "launches",
+        "bricks_hinted", "bricks_staged")] + \
         [(n, C.c_double) for n in ("ms_last_frame", "ms_stall_last_frame", "bytes_h2d_last_frame",
                                    "ms_trace_last_frame", "ms_prefetch_last_frame")]
 

@@ -246,10 +246,12 @@ vt_status BrickCache::prefetch_stage(const std::vector<uint64_t>& bricks, std::v
                                       std::vector<int>& hslot) {
     staged.clear();
     const size_t cap = (size_t)std::min(nSlots_, nHost_);
+    hinted_ += (int64_t)bricks.size();
     for (uint64_t b : bricks) {
         if (staged.size() >= cap) break;
         if (pageMirror_[b - pageBase_] < 0) staged.push_back(b);
     }
+    staged_ += (int64_t)staged.size();
     if (staged.empty()) { hslot.clear(); return VT_OK; }
     int64_t disk = 0;
     return ensure_host(staged, hslot, &disk);
@@ -305,6 +307,7 @@ void BrickCache::fold_stats(vt_stats& st) {
     st.host_hits = hostHits_; st.host_misses = hostMisses_;
     st.bricks_requested = requested_; st.bricks_loaded_disk = hostMisses_;
     st.bricks_loaded_host = hostHits_; st.bricks_prefetched = prefetched_;
+    st.bricks_hinted = hinted_; st.bricks_staged = staged_;
     st.launches += launches_ - launchesFolded_;
     launchesFolded_ = launches_;
 }
@@ -322,6 +325,6 @@ vt_status BrickCache::drop() {
     return VT_OK;
 }
 
-void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = 0; }
+void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = 0; }
 
 }  // namespace vtrt

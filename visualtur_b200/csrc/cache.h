@@ -89,7 +89,7 @@ private:
     unsigned int pass_ = 0, frameStart_ = 1;
     bool allResident_ = false;
     /* stats */
-    int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0;
+    int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0, hinted_ = 0, staged_ = 0;
     int64_t launches_ = 0, launchesFolded_ = 0;
 };
 

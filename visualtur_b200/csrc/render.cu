@@ -72,10 +72,16 @@ __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
  * fetched per round: their positions accumulate in the reference's order,
  * their taps are issued together, and the crossing test then runs sample
  * by sample -- fetches past the hit are discarded (indices stay clamped to
- * the brick) and are not counted. */
+ * the brick) and are not counted.
+ *
+ * refine > 0 bisects the bracketing pair [previous, current sample] that
+ * many times before the linear step: the midpoint replaces the end whose
+ * iso - value has the same strict sign as its own (the crossing test's
+ * "no crossing" condition), so the pair keeps bracketing the crossing.
+ * Each midpoint is one more trilinear sample. */
 template <int VTYPE, int U>
 __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, float tnear,
-                                      int maxStep, float iso, float3* Xhit, unsigned int* nsamp) {
+                                      int maxStep, float iso, int refine, float3* Xhit, unsigned int* nsamp) {
     float3 Xnear = add(origin, mul(ray, tnear));
     float3 Xfar = Xnear;
     float3 vStep = mul(ray, 0.5f);
@@ -100,8 +106,20 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
                 ant = sig;
                 Xfar = X[u];
             } else {
+                float3 P = Xfar, Q = X[u];
+                for (int k = 0; k < refine; k++) {
+                    float3 M = mul(add(P, Q), 0.5f);
+                    float vm = interp<VTYPE>(s, M);
+                    ns++;
+                    if ((((iso - ant) < 0.0f) && ((iso - vm) < 0.0f)) ||
+                        (((iso - ant) > 0.0f) && ((iso - vm) > 0.0f))) {
+                        P = M; ant = vm;
+                    } else {
+                        Q = M; sig = vm;
+                    }
+                }
                 float a = (iso - ant) / (sig - ant);
-                *Xhit = add(mul(Xfar, 1.0f - a), mul(X[u], a));
+                *Xhit = add(mul(P, 1.0f - a), mul(Q, a));
                 hit = true;
             }
         }
@@ -304,7 +322,7 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
         if (!slab(R.r, mbx, mby, mbz, mbx + dimO, mby + dimO, mbz + dimO, &tn, &tf)) continue;
         float3 X;
         unsigned int ns = 0;
-        bool h = march<VTYPE, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, &X, &ns);
+        bool h = march<VTYPE, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
         cnt[VT_C_SAMPLES] += ns;
         if (h) {
             /* shade (src/rayCaster.cu:238-250) */

@@ -331,6 +331,7 @@ extern "C" void vt_default_options(vt_options* o) {
     o->pops = 8;
     o->preload = 1;
     o->use_graph = 1;
+    o->refine = 0;
 }
 
 static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
@@ -348,6 +349,7 @@ static vt_status validate(const vt_params* p, const vt_octree* o, const vt_optio
         if (tw <= 0 || th <= 0 || tw * th > 4096) return fail(VT_ERR_INVALID, "tile %dx%d: 1..4096 rays", tw, th);
         if (opt->unroll != 1 && opt->unroll != 2 && opt->unroll != 4 && opt->unroll != 8)
             return fail(VT_ERR_INVALID, "unroll must be 1, 2, 4 or 8");
+        if (opt->refine < 0 || opt->refine > 16) return fail(VT_ERR_INVALID, "refine must be in 0..16");
         if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
             return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
     }
@@ -528,6 +530,7 @@ static void fill_args(vt_handle* h, TraceArgs& a, int nViews, unsigned int total
     a.tile_w = h->opt.tile_w; a.tile_h = h->opt.tile_h;
     a.pops = h->opt.pops > 0 ? h->opt.pops : 8;
     a.unroll = h->opt.unroll;
+    a.refine = h->opt.refine;
 }
 
 static vt_status collect_counters(vt_handle* h, cudaStream_t s) {

@@ -114,6 +114,7 @@ struct TraceArgs {
     int tile_w, tile_h;
     int pops;                                   /* pops between warp refills (persistent) */
     int unroll;                                 /* march samples fetched per round: 1, 2, 4, 8 */
+    int refine;                                 /* bisection steps before the linear refinement */
 };
 
 /* launchers (render.cu) */

@@ -82,7 +82,13 @@ __device__ __forceinline__ bool slab_t(float tmin, float tmax, float tymin, floa
 
 /* Level of a sentinel-bit Morton code (getIndexLevel,
  * inc/mortonCodeUtil.hpp:42-86) for valid codes (>= 1). */
-__device__ __forceinline__ int code_level(uint64_t c) { return (63 - __clzll((long long)c)) / 3; }
+VT_HD int code_level(uint64_t c) {
+#ifdef __CUDA_ARCH__
+    return (63 - __clzll((long long)c)) / 3;
+#else
+    return (63 - __builtin_clzll(c)) / 3;
+#endif
+}
 
 /* Inverse of the 3-way bit dilation: bit 3k of v -> bit k. */
 VT_HD uint32_t compact3(uint64_t v) {

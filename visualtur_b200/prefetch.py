@@ -114,6 +114,9 @@ class Prefetcher:
         self.n, self.fov, self.levelC, self.level = n, fov, levelC, level
         self.mlp = MLP((FEATURES, hidden, hidden, 8 ** level), seed=seed)
         self.groups = node_bricks(brick_list, levelC, level)
+        # bricks with the coarse node each lies in, for vectorised selection
+        self.bricks = np.sort(np.asarray(brick_list, np.uint64))
+        self.brick_node = ((self.bricks >> np.uint64(3 * (levelC - level))) - np.uint64(8 ** level)).astype(np.int64)
 
     def train(self, torch, X, Y, epochs=30, batch=256, lr=1e-3, seed=0):
         """X: N x 12 features, Y: N x 8^level targets; returns per-epoch loss"""
@@ -140,9 +143,8 @@ class Prefetcher:
         return p.cpu().numpy().reshape(f.shape[0], -1)
 
     def bricks_for(self, probs, threshold):
-        nodes = np.flatnonzero(probs > threshold)
-        parts = [self.groups[int(k)] for k in nodes if int(k) in self.groups]
-        return np.concatenate(parts) if parts else np.zeros(0, np.uint64)
+        """sorted brick codes of every node whose probability exceeds threshold"""
+        return self.bricks[np.asarray(probs)[self.brick_node] > threshold]
 
 
 def collect_traces(renderer, n, W, H, fov, rng, paths, frames, r_lo, r_hi, level=TRACE_LEVEL, dist=50.0):
