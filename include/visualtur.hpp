@@ -63,7 +63,7 @@ public:
     }
     int CreateFile(float* volume, char* newname, char* dataset_name, int x, int y, int z) {
         int64_t d[3] = {x, y, z};
-        check(vt_volume_write(newname, dataset_name, 0, volume, VT_F32, d));
+        check(vt_volume_write(newname, dataset_name, 1, volume, VT_F32, d));
         return 0;
     }
     vt_volume* handle() const { return v_; }

@@ -55,8 +55,12 @@ enum { VT_F32 = 0, VT_U8 = 1 };
 typedef struct vt_volume vt_volume;
 
 /* FileManager::FileManager (src/FileManager.cu:11-37).  Opens a project raw
- * volume file ("VTVOL001" header) or an HDF5 file holding one contiguous
- * 3-D dataset; `dataset` names the HDF5 dataset (ignored for raw files). */
+ * volume file ("VTVOL001" header) or an HDF5 file holding a contiguous or
+ * compact 3-D dataset; `dataset` is its path in the file ("value",
+ * "/grp/value"; ignored for raw files).  float32 and uint8 datasets are
+ * memory-mapped; other little-endian integer or float datasets are
+ * converted to float32 in memory, as the reference's H5Dread to
+ * H5T_IEEE_F32LE converts them (src/FileManager.cu:155). */
 vt_status vt_volume_open(const char* path, const char* dataset, vt_volume** out);
 /* Wraps caller-owned host memory as a volume (no copy; must outlive it). */
 vt_status vt_volume_wrap(const void* data, int vtype, const int64_t dims[3], vt_volume** out);
@@ -72,6 +76,17 @@ vt_status vt_volume_read_all(const vt_volume* v, void* out);
  * 1 = HDF5 (contiguous dataset named `dataset`). */
 vt_status vt_volume_write(const char* path, const char* dataset, int format, const void* data,
                           int vtype, const int64_t dims[3]);
+
+/* HDF5 dataset inspection (no reference counterpart): how libvt's reader
+ * sees the dataset `dataset` of the HDF5 file `path`.  type_class: 0 fixed
+ * point, 1 IEEE float; offset: file offset of the first element. */
+typedef struct {
+    int rank;
+    int64_t dims[32];
+    int type_class, type_size, is_signed, big_endian;
+    uint64_t offset, bytes;
+} vt_h5_info;
+vt_status vt_h5_describe(const char* path, const char* dataset, vt_h5_info* out);
 
 /* Seeded synthetic volumes (no reference counterpart).
  *   VT_GEN_SPHERE: |x-c| + 0.25*g, g ~ N(0,1) by 4-term Irwin-Hall;

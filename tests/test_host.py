@@ -95,11 +95,11 @@ def test_error_statuses(workdir):
 def test_raw_volume_roundtrip(workdir):
     vol = F.case_volume("s64")
     path = os.path.join(workdir, "rt.raw")
-    vt.FileManager.CreateFile(vol, path)
+    vt.FileManager.CreateFile(vol, path, fmt=0)
     fm = vt.FileManager(path)
     assert fm.dims == (64, 64, 64) and np.array_equal(fm.readHDF5(), vol)
     u8 = (np.arange(4 * 5 * 6) % 251).astype(np.uint8).reshape(4, 5, 6)
-    vt.FileManager.CreateFile(u8, path)
+    vt.FileManager.CreateFile(u8, path, fmt=0)
     fm = vt.FileManager(path)
     assert fm.vtype == vt.VT_U8 and np.array_equal(fm.readHDF5(), u8)
     assert np.array_equal(fm.readHDF5_Voxel_Array((-1, 0, 2), (3, 5, 8)),

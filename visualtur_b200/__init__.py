@@ -62,6 +62,11 @@ class vt_stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class vt_h5_info(C.Structure):
+    _fields_ = [("rank", C.c_int), ("dims", C.c_int64 * 32), ("type_class", C.c_int), ("type_size", C.c_int),
+                ("is_signed", C.c_int), ("big_endian", C.c_int), ("offset", C.c_uint64), ("bytes", C.c_uint64)]
+
+
 class vt_tuning(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("tile_w", "tile_h", "unroll", "persistent", "pops", "blocks_per_sm",
                                          "lookahead", "use_graph")]
@@ -87,6 +92,7 @@ _PROTOS = {
     "vt_volume_read": (C.c_int, [_P, C.c_int * 3, C.c_int * 3, _P]),
     "vt_volume_read_all": (C.c_int, [_P, _P]),
     "vt_volume_write": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, _P, C.c_int, _I64_3]),
+    "vt_h5_describe": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(vt_h5_info)]),
     "vt_generate_volume": (C.c_int, [C.c_int, C.c_uint64, _I64_3, _P, C.c_int, _P]),
     "vt_generate_volume_device": (C.c_int, [C.c_int, C.c_uint64, _I64_3, _P, C.c_int, _P, _P]),
     "vt_octree_load": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
@@ -215,10 +221,23 @@ class FileManager:
         return out
 
     @staticmethod
-    def CreateFile(volume, newname, dataset_name="value", fmt=0):
+    def CreateFile(volume, newname, dataset_name="value", fmt=1):
+        """Writes the volume as an HDF5 file with one contiguous dataset
+        (fmt 1, as FileManager::CreateFile) or as a raw VTVOL001 file (fmt 0)."""
         a = np.ascontiguousarray(volume)
         vt = VT_U8 if a.dtype == np.uint8 else VT_F32
         check(lib().vt_volume_write(newname.encode(), dataset_name.encode(), fmt, a.ctypes.data, vt, _d3(a.shape)))
+
+    @staticmethod
+    def h5_describe(path, dataset="value"):
+        """The HDF5 dataset as libvt's reader sees it: rank, dims, element
+        class ("int"/"float"), size, signedness, byte order, file offset."""
+        i = vt_h5_info()
+        check(lib().vt_h5_describe(path.encode(), dataset.encode(), C.byref(i)))
+        return {"rank": i.rank, "dims": tuple(int(i.dims[k]) for k in range(i.rank)),
+                "class": "float" if i.type_class == 1 else "int", "size": i.type_size,
+                "signed": bool(i.is_signed), "big_endian": bool(i.big_endian),
+                "offset": int(i.offset), "bytes": int(i.bytes)}
 
     def close(self):
         if self._h:

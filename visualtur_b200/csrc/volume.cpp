@@ -102,12 +102,63 @@ extern "C" vt_status vt_volume_open(const char* path, const char* dataset, vt_vo
     const unsigned char* p = (const unsigned char*)base;
     int vtype; int64_t dims[3]; uint64_t off;
     std::string why;
+    H5Dataset h5;
+    bool convert = false;
     bool ok = parse_raw(p, len, &vtype, dims, &off);
-    if (!ok) ok = h5_locate(p, len, dataset ? dataset : "value", &vtype, dims, &off, &why);
+    if (!ok && h5_describe(p, len, dataset ? dataset : "value", &h5, &why)) {
+        ok = true;
+        if (h5.rank != 3) { ok = false; why = "dataset is not 3-D"; }
+        else if (h5.big_endian) { ok = false; why = "big-endian datasets are not supported"; }
+        else if (h5.type_class == 1 && h5.type_size == 4) vtype = VT_F32;
+        else if (h5.type_class == 0 && h5.type_size == 1 && !h5.is_signed) vtype = VT_U8;
+        else if ((h5.type_class == 1 && h5.type_size == 8) ||
+                 (h5.type_class == 0 && (h5.type_size == 1 || h5.type_size == 2 || h5.type_size == 4 ||
+                                         h5.type_size == 8))) { vtype = VT_F32; convert = true; }
+        else { ok = false; why = "unsupported voxel type"; }
+        for (int a = 0; a < 3; a++) dims[a] = h5.dims[a];
+        off = h5.offset;
+    }
     if (!ok) {
         munmap(base, len);
         return fail(VT_ERR_FORMAT, "unable to open the requested data set in %s: %s", path,
                     why.empty() ? "not a raw volume or HDF5 file" : why.c_str());
+    }
+    if (convert) {
+        size_t n = (size_t)dims[0] * dims[1] * dims[2];
+        if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0 || off + n * h5.type_size > len) {
+            munmap(base, len);
+            return fail(VT_ERR_FORMAT, "truncated volume %s", path);
+        }
+        vt_volume* v = new vt_volume();
+        v->vtype = VT_F32;
+        for (int a = 0; a < 3; a++) v->dims[a] = dims[a];
+        v->owned.resize(n * 4);
+        float* dst = (float*)v->owned.data();
+        const unsigned char* src = p + off;
+        const int es = h5.type_size;
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)n; i++) {
+            const unsigned char* e = src + (size_t)i * es;
+            float f;
+            if (h5.type_class == 1) { double x; memcpy(&x, e, 8); f = (float)x; }
+            else if (h5.is_signed) {
+                if (es == 1) f = (float)(int8_t)e[0];
+                else if (es == 2) { int16_t x; memcpy(&x, e, 2); f = (float)x; }
+                else if (es == 4) { int32_t x; memcpy(&x, e, 4); f = (float)x; }
+                else { int64_t x; memcpy(&x, e, 8); f = (float)x; }
+            } else {
+                if (es == 1) f = (float)e[0];
+                else if (es == 2) { uint16_t x; memcpy(&x, e, 2); f = (float)x; }
+                else if (es == 4) { uint32_t x; memcpy(&x, e, 4); f = (float)x; }
+                else { uint64_t x; memcpy(&x, e, 8); f = (float)x; }
+            }
+            dst[i] = f;
+        }
+        munmap(base, len);
+        v->data = v->owned.data();
+        v->path = path;
+        *out = v;
+        return VT_OK;
     }
     size_t need = (size_t)dims[0] * dims[1] * dims[2] * (vtype == VT_U8 ? 1 : 4);
     if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0 || off + need > len) {
@@ -120,6 +171,31 @@ extern "C" vt_status vt_volume_open(const char* path, const char* dataset, vt_vo
     v->map_base = base; v->map_len = len; v->data = p + off; v->path = path;
     madvise(base, len, MADV_WILLNEED);
     *out = v;
+    return VT_OK;
+}
+
+extern "C" vt_status vt_h5_describe(const char* path, const char* dataset, vt_h5_info* out) {
+    clear_error();
+    if (!path || !out) return fail(VT_ERR_INVALID, "vt_h5_describe: null argument");
+    int fd = open(path, O_RDONLY);
+    if (fd < 0) return fail(VT_ERR_IO, "unable to open the requested file %s", path);
+    struct stat st;
+    if (fstat(fd, &st) != 0 || st.st_size < 8) { close(fd); return fail(VT_ERR_FORMAT, "file too small: %s", path); }
+    size_t len = (size_t)st.st_size;
+    void* base = mmap(nullptr, len, PROT_READ, MAP_SHARED, fd, 0);
+    close(fd);
+    if (base == MAP_FAILED) return fail(VT_ERR_IO, "mmap failed: %s", path);
+    H5Dataset d;
+    std::string why;
+    bool ok = h5_describe((const unsigned char*)base, len, dataset ? dataset : "value", &d, &why);
+    munmap(base, len);
+    if (!ok) return fail(VT_ERR_FORMAT, "%s: %s", path, why.c_str());
+    memset(out, 0, sizeof(*out));
+    out->rank = d.rank;
+    for (int k = 0; k < d.rank && k < 32; k++) out->dims[k] = d.dims[k];
+    out->type_class = d.type_class; out->type_size = d.type_size;
+    out->is_signed = d.is_signed; out->big_endian = d.big_endian;
+    out->offset = d.offset; out->bytes = d.bytes;
     return VT_OK;
 }
 

@@ -57,9 +57,18 @@ void volume_read_native(const vt_volume* v, const int s[3], const int e[3], void
 int children_mask(const uint64_t* e, int size, uint64_t father);
 /* reference host-variant child count (src/CreateOctree.cu:247-284) */
 int search_children_host(const uint64_t* e, int64_t size, uint64_t father);
-/* h5lite: locate the contiguous 3-D dataset of an HDF5 file */
-bool h5_locate(const unsigned char* file, size_t len, const char* dataset, int* vtype,
-               int64_t dims[3], uint64_t* offset, std::string* why);
+/* h5lite: a dataset of an HDF5 file as stored */
+struct H5Dataset {
+    int rank = 0;
+    int64_t dims[32] = {0};
+    int type_class = -1;        /* 0 fixed point, 1 IEEE float */
+    int type_size = 0;          /* bytes per element */
+    bool is_signed = false, big_endian = false;
+    uint64_t offset = 0;        /* file offset of element 0 */
+    uint64_t bytes = 0;         /* storage size */
+    bool offset_is_addr = false;
+};
+bool h5_describe(const unsigned char* file, size_t len, const char* path, H5Dataset* d, std::string* why);
 bool h5_write(const char* path, const char* dataset, const void* data, int vtype, const int64_t dims[3],
               std::string* why);
 }  // namespace vtrt
