@@ -1,10 +1,10 @@
 #!/usr/bin/env python
 """Benchmark: rays/s and ms/frame of the isosurface ray caster on B200.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1|c2s] [--mode best|plain]
-                  [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1|c3|c2s|c3s]
+                  [--mode best|plain] [--impl ours|reference]
 
-A step is one rendered frame of the workload:
+A step is one rendered frame of the workload (one batch of views for c3):
   c2 (default): the 2048^3 float32 out-of-core fly-through -- 256 seeded
       anisotropic Gaussian blobs + 4-octave value noise, isovalue 0.6,
       16^3 bricks (apron 3), device brick cache 4 GB, pinned host tier
@@ -12,6 +12,11 @@ A step is one rendered frame of the workload:
       Inputs exceed L2 (32 GB volume), no flush between frames.
   c1: the 128^3 noisy sphere, fully resident in HBM, one 512x512 camera at
       distance 300; L2 flushed (256 MB write) between timed frames.
+  c3: the c2 volume, 64 seeded views per launch at random poses on a
+      sphere of radius 2500-3500 looking into the inner half, resolutions
+      drawn from {256^2, 512^2, 1024^2, 1920x1080, 2048^2}; the autotuner
+      also picks the brick edge {8, 16, 32}.
+  c2s / c3s: c2 / c3 on a 1024^3 volume (profiling and quick checks).
 value = rays of all ranks / device time (CUDA events, max over ranks).
 Multi-GPU: replicas only -- each rank renders its own frames, no
 collective on the data path ("scaling": "weak").
@@ -48,6 +53,24 @@ CONFIGS = {
                gen="blobs", seed=2048, n=2048, iso=0.6, levelC=7, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
                dist=50.0, resident=0, l2flush=False, orbit=(3000.0, 1.2), dev_bytes=4 << 30,
                host_bytes=16 << 30, blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05)),
+    # 64 seeded views per launch, mixed resolutions, on the c2 volume
+    "c3": dict(workload="2048^3 f32 blobs+noise (the c2 volume), 64 views per launch at seeded random poses "
+                        "on a sphere r in [2500,3500] looking into the inner half, resolutions drawn from "
+                        "{256^2, 512^2, 1024^2, 1920x1080, 2048^2}; 4 GB device cache, 16 GB pinned host tier, "
+                        "timed from a cold cache",
+               gen="blobs", seed=2048, n=2048, iso=0.6, levelC=7, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
+               dist=50.0, resident=0, l2flush=False, orbit=None, dev_bytes=4 << 30, host_bytes=16 << 30,
+               blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05),
+               views=dict(n=64, r=(2500.0, 3500.0), res=((256, 256), (512, 512), (1024, 1024), (1920, 1080),
+                                                         (2048, 2048)))),
+    # c3 on the 1 GB volume (quick checks)
+    "c3s": dict(workload="1024^3 f32 blobs+noise (c2 scaled by 1/2), 64 views per launch, r in [1250,1750], "
+                         "mixed resolutions as c3",
+                gen="blobs", seed=2048, n=1024, iso=0.6, levelC=6, levelO=8, inc=3, W=1920, H=1080, fov=30.0,
+                dist=50.0, resident=0, l2flush=False, orbit=None, dev_bytes=2 << 30, host_bytes=4 << 30,
+                blobs=(256, 10.0, 60.0, 0.5, 1.5, 0.05),
+                views=dict(n=64, r=(1250.0, 1750.0), res=((256, 256), (512, 512), (1024, 1024), (1920, 1080),
+                                                          (2048, 2048)))),
     # profiling-sized version of c2 (1 GB volume) for ncu captures
     "c2s": dict(workload="1024^3 f32 blobs+noise (c2 scaled by 1/2), iso 0.6, 16^3 bricks, 1920x1080, orbit r=1500",
                 gen="blobs", seed=2048, n=1024, iso=0.6, levelC=6, levelO=8, inc=3, W=1920, H=1080, fov=30.0,
@@ -135,6 +158,24 @@ def frame_camera(vt, cfg, frame):
     return orbit_camera(vt, cfg, frame) if cfg["orbit"] else static_camera(vt, cfg)
 
 
+def step_views(cfg, step):
+    """The seeded views of one batched step: positions uniform on a sphere
+    shell around the volume centre, targets uniform in the inner half,
+    resolution drawn uniformly from the config's list."""
+    from visualtur_b200 import prefetch as pf
+    spec, n = cfg["views"], cfg["n"]
+    rng = np.random.default_rng([cfg["seed"], 3, step])
+    c = (n - 1) / 2.0
+    out = []
+    for _ in range(spec["n"]):
+        v = rng.standard_normal(3)
+        pos = c + v / np.linalg.norm(v) * rng.uniform(*spec["r"])
+        tgt = c + rng.uniform(-n / 4.0, n / 4.0, 3)
+        W, H = spec["res"][int(rng.integers(len(spec["res"])))]
+        out.append(pf.look_at(W, H, cfg["dist"], cfg["fov"], pos, tgt))
+    return out
+
+
 class Workload:
     """Volume (device generated), octree (GPU builder) and renderer."""
 
@@ -167,27 +208,33 @@ class Workload:
         if need_renderer:
             self.fm = vt.FileManager.wrap(self.volume)
             self.oc = vt.Octree(self.octree_path)
-            edge = 1 << (self.oc.nLevels - cfg["levelC"])
-            D = edge + 2 * cfg["inc"]
-            slot = (D ** 3 * 4 + 15) // 16 * 16
-            dev = cfg.get("dev_bytes", 0) // slot or 8 ** cfg["levelC"]
-            host = cfg.get("host_bytes", 0) // slot or 8 ** cfg["levelC"]
-            self.slots = (dev, host, slot)
-            p = vt.make_params(W=cfg["W"], H=cfg["H"], octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"],
-                               levelCubes=cfg["levelC"], dimCube=edge, cubeInc=cfg["inc"], distance=cfg["dist"],
-                               fov_H=cfg["fov"], fov_W=cfg["fov"], maxElementsCache=dev, maxElementsCache_CPU=host)
-            self.params = p
+            self.brick = 1 << (self.oc.nLevels - cfg["levelC"])
             t4 = time.time()
             self.r = self.renderer(mode, warm)
-            log("setup: renderer %.1fs (device slots %d, host slots %d, %d B/brick)" % (time.time() - t4, dev, host, slot))
+            log("setup: renderer %.1fs (device slots %d, host slots %d, %d B/brick)" %
+                ((time.time() - t4,) + self.slots))
 
+    def params(self, brick=None):
+        """Renderer parameters for brick edge `brick` (default: the config's
+        levelCubes); cache slots from the config's device / host bytes."""
+        vt, cfg = self.vt, self.cfg
+        edge = brick or self.brick
+        levelC = self.oc.nLevels - int(round(math.log2(edge)))
+        D = edge + 2 * cfg["inc"]
+        slot = (D ** 3 * 4 + 15) // 16 * 16
+        dev = cfg.get("dev_bytes", 0) // slot or 8 ** levelC
+        host = cfg.get("host_bytes", 0) // slot or 8 ** levelC
+        self.slots = (dev, host, slot)
+        return vt.make_params(W=cfg["W"], H=cfg["H"], octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"],
+                              levelCubes=levelC, dimCube=edge, cubeInc=cfg["inc"], distance=cfg["dist"],
+                              fov_H=cfg["fov"], fov_W=cfg["fov"], maxElementsCache=dev, maxElementsCache_CPU=host)
 
-    def renderer(self, mode, warm=False):
+    def renderer(self, mode, warm=False, brick=None):
         """A renderer in `mode` (cold cache unless the workload is resident
         or `warm`: every needed brick preloaded, for steady-state profiles)."""
         opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=0,
                                       preload=1 if (self.cfg["resident"] or warm) else 0, **MODES[mode]["opts"])
-        return self.vt.visualTur(self.params, opt, volume=self.fm, octree=self.oc)
+        return self.vt.visualTur(self.params(brick), opt, volume=self.fm, octree=self.oc)
 
     def train_prefetcher(self, torch, poses=20000, paths=100, W=240, H=135, epochs=30):
         """Learned prefetch: traces from random fly-throughs (radius
@@ -234,22 +281,28 @@ def roofline(stats_frames, trace_ms, pixels):
         pass
     ach = b_alg / (trace_ms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "peak_source": src, "unit": "GB/s",
-            "frac": round(ach / peak, 4), "traffic": None, "bytes_alg_per_frame": b_alg / len(stats_frames),
+            "frac": round(ach / peak, 4), "traffic": None, "bytes_alg_per_launch": b_alg / len(stats_frames),
             "kernel": "k_trace"}
 
 
-def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, frame=0):
-    """Oracle (CPU restatement of the reference algorithm) on a bounded ray
-    sample of frame `frame`; returns rays/s."""
-    from oracle import oracle as orc
+def sample_camera(cfg, step):
+    """The camera the CPU baseline renders for `step`: the frame's camera,
+    or the first view of a batched step."""
     import visualtur_b200 as vt
+    return step_views(cfg, step)[0] if "views" in cfg else frame_camera(vt, cfg, step)
+
+
+def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0):
+    """Oracle (CPU restatement of the reference algorithm) on a bounded ray
+    sample of step `step`'s camera; returns rays/s."""
+    from oracle import oracle as orc
     o = orc.Octree(octree_path)
-    c = frame_camera(vt, cfg, frame)
-    cam = orc.Camera(cfg["H"], cfg["W"], cfg["dist"], cfg["fov"], cfg["fov"])
+    c = sample_camera(cfg, step)
+    cam = orc.Camera(c.H, c.W, cfg["dist"], cfg["fov"], cfg["fov"])
     for f in ("look", "up", "right", "position"):
         v = getattr(c, f)
         setattr(cam.c, f, orc.orc_f3(v[0], v[1], v[2]))
-    n = cfg["W"] * cfg["H"]
+    n = c.W * c.H
     stride = 1
     # probe a sparse sample, then size the sample to the time budget
     t0 = time.perf_counter()
@@ -269,7 +322,8 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, frame=0):
     el = time.perf_counter() - t0
     threads = nthreads or os.cpu_count()
     return {"value": round(rays / el, 1), "unit": "rays/s", "cores": threads, "kind": "port",
-            "sample": "%d x every %d-th ray of frame %d (%d rays, %.1f s)" % (reps, stride, frame, rays, el)}
+            "sample": "%d x every %d-th ray of a %dx%d view of step %d (%d rays, %.1f s)" %
+                      (reps, stride, c.W, c.H, step, rays, el)}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -289,6 +343,13 @@ class Launcher:
 
     def cams(self, f0, n):
         return [frame_camera(self.wl.vt, self.cfg, f0 + i) for i in range(n)]
+
+    def rays(self, cams):
+        return sum(c.W * c.H for c in cams)
+
+    def outputs(self, cams):
+        """(device RGB8 buffer, bytes) of each frame of the last launch"""
+        return [(self.bufs[b][1], c.W * c.H * 3) for b, c in enumerate(cams)]
 
     def hint(self, cams):
         if self.P is None or not cams:
@@ -313,12 +374,58 @@ class Launcher:
         self.r.render_batch(views, stream=sp)
 
 
+class ViewLauncher:
+    """Batched workload: each step is one launch of that step's views (mixed
+    resolutions, RGB8 output); `plain` renders the same views one per launch
+    instead.  With a predictor, the hint names the predicted bricks of this
+    step's and the next step's views."""
+    batch = 1
+
+    def __init__(self, wl, r, cfg, torch, dev, stream, predictor=None, threshold=0.25, warm=False, plain=False):
+        self.wl, self.r, self.cfg, self.torch, self.stream = wl, r, cfg, torch, stream
+        self.warm, self.plain, self.P, self.thr = warm, plain, predictor, threshold
+        spec = cfg["views"]
+        maxpix = max(w * h for w, h in spec["res"])
+        self.bufs = [torch.empty(maxpix * 3, dtype=torch.uint8, device=dev) for _ in range(spec["n"])]
+
+    def cams(self, f0, n):
+        return [step_views(self.cfg, f0 + i) for i in range(n)]
+
+    def rays(self, items):
+        return sum(c.W * c.H for views in items for c in views)
+
+    def outputs(self, items):
+        return [(b, c.W * c.H * 3) for c, b in zip(items[-1], self.bufs)]
+
+    def hint(self, items):
+        if self.P is None or not items:
+            return
+        from visualtur_b200 import prefetch as pf
+        feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for views in items for c in views])
+        probs = self.P.predict(self.torch, feats).max(axis=0)
+        self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
+
+    def launch(self, items, next_items=()):
+        self.hint(list(items) + list(next_items))
+        sp = self.stream.cuda_stream
+        views = []
+        for c, b in zip(items[0], self.bufs):
+            v = self.wl.vt.vt_view()
+            v.cam, v.dev_rgba, v.dev_rgb8 = c, None, b.data_ptr()
+            views.append(v)
+        if self.plain:
+            for v in views:
+                self.r.render_batch([v], stream=sp)
+        else:
+            self.r.render_batch(views, stream=sp)
+
+
 def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
     """Renders `warmup` then `steps` consecutive frames in launches of
     L.batch; returns device ms (CUDA events on the launching stream) and
     stats per launch, and the number of frames in each."""
     torch, r, stream = L.torch, L.r, L.stream
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=L.bufs[0][0].device) if flush_l2 else None
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=stream.device) if flush_l2 else None
     with torch.cuda.stream(stream):
         f = frame0
         while f < frame0 + warmup:
@@ -355,7 +462,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
         if dist:
             dist.barrier()
     clk = clocks.stop() if clocks else None
-    return [a.elapsed_time(b) for a, b in ev], per, [n for _, n, _, _ in launches], clk
+    return [a.elapsed_time(b) for a, b in ev], per, launches, clk
 
 
 def frame_deltas(per_frame):
@@ -366,34 +473,71 @@ def frame_deltas(per_frame):
     return out
 
 
+def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=False, plain=False):
+    if "views" in cfg:
+        return ViewLauncher(wl, r, cfg, torch, dev, stream, predictor=predictor, warm=warm, plain=plain)
+    return Launcher(wl, r, cfg, torch, dev, stream, batch=batch, predictor=predictor, warm=warm)
+
+
+def autotune(args, wl, cfg, torch, dev, stream, frame0, batch):
+    """Kernel schedule sweep (tile x unroll x persistent) on the renderer;
+    for the batched workload first the brick edge {8, 16, 32} at the
+    default schedule, keeping the fastest renderer."""
+    from visualtur_b200 import autotune as at
+    bricks = None
+    if "views" in cfg and not args.no_brick_sweep:
+        L0 = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch)
+        items = L0.cams(frame0, 1)
+        rows = []
+        for b in (8, 16, 32):
+            r = wl.r if b == wl.brick else wl.renderer(args.mode, brick=b)
+            L = make_launcher(wl, r, cfg, torch, dev, stream, batch)
+            ms = at.time_frames(torch, r, lambda rr, i, s_: L.launch(items), frames=1, warmup=1, stream=stream)
+            rows.append({"brick": b, "ms": round(ms, 3)})
+            log("autotune: brick %d -> %.2f ms" % (b, ms))
+            if r is not wl.r:
+                r.close()
+        best_b = min(rows, key=lambda x: x["ms"])["brick"]
+        if best_b != wl.brick:
+            wl.r.close()
+            wl.brick = best_b
+            wl.r = wl.renderer(args.mode)
+        bricks = rows
+    Lt = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch)
+    items = Lt.cams(frame0, batch)
+    frames = 1 if "views" in cfg else 3
+    best, table = at.tune_schedule(torch, wl.r, lambda rr, i, s_: Lt.launch(items), frames=frames, stream=stream)
+    if bricks:
+        best = dict(best, brick=wl.brick)
+    log("autotune: best %s" % best)
+    if not cfg["resident"]:
+        wl.r.drop_cache()
+    return {"best": best, "points": len(table) + len(bricks or []), "bricks": bricks, "table": table}
+
+
 def run_ours(args, cfg, rank, world, torch, dist):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     work = tempfile.mkdtemp(prefix="vtbench_")
     M = MODES[args.mode]
     wl = Workload(cfg, torch, dev, work, mode=args.mode, warm=args.warm)
-    W, H = cfg["W"], cfg["H"]
     stream = torch.cuda.Stream(device=dev)
     frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
-    batch = 1 if cfg["resident"] else M["batch"]
+    batch = 1 if (cfg["resident"] or "views" in cfg) else M["batch"]
     P = wl.train_prefetcher(torch) if (M["learned"] and not cfg["resident"] and not args.no_learned) else None
     tune = None
     if M["autotune"] and not args.no_autotune:
-        from visualtur_b200 import autotune as at
-        Ltune = Launcher(wl, wl.r, cfg, torch, dev, stream, batch=batch)
-        cams = Ltune.cams(frame0, batch)
-        best, table = at.tune_schedule(torch, wl.r, lambda rr, i, s_: Ltune.launch(cams), frames=3, stream=stream)
-        tune = {"best": best, "points": len(table), "table": table}
-        log("autotune: best %s" % best)
-        if not cfg["resident"]:
-            wl.r.drop_cache()
-    L = Launcher(wl, wl.r, cfg, torch, dev, stream, batch=batch, predictor=P, warm=args.warm)
-    ms, per, nfr, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index), cfg["l2flush"])
+        tune = autotune(args, wl, cfg, torch, dev, stream, frame0, batch)
+    if P is not None:
+        P.set_bricks(wl.r.brick_list(), wl.oc.nLevels - int(round(math.log2(wl.brick))))
+    L = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch, predictor=P, warm=args.warm)
+    ms, per, launches, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index),
+                                          cfg["l2flush"])
     tot_ms = sum(ms)
     st = wl.r.stats()
     ld = frame_deltas(per)
     trace_tot = sum(s["ms_trace_last_frame"] for s in per)
-    rays_rank = W * H * args.steps
+    rays_rank = sum(L.rays(cams) for _, _, cams, _ in launches)
     t_max = tot_ms
     if dist:
         t = torch.tensor([tot_ms], device=dev)
@@ -401,31 +545,37 @@ def run_ours(args, cfg, rank, world, torch, dist):
         t_max = float(t.item())
     value = rays_rank * world / (t_max * 1e-3)
     # end to end through the public API: poses in, RGB8 images back in pinned host memory
-    e2e_frames = max(batch, 2 * batch if batch > 1 else 30)
-    host8 = [torch.empty(W * H * 3, dtype=torch.uint8, pin_memory=True) for _ in range(batch)]
+    e2e_steps = max(batch, 2 * batch if batch > 1 else (4 if "views" in cfg else 30))
+    maxb = max(b.numel() for b, _ in L.outputs(L.cams(frame0, batch)))
+    host8 = [torch.empty(maxb, dtype=torch.uint8, pin_memory=True) for _ in range(64)]
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
     f = frame0 + args.warmup + args.steps
+    e2e_rays = d2h = h2d = 0
+    t0 = time.perf_counter()
     with torch.cuda.stream(stream):
-        for k in range(0, e2e_frames, batch):
+        for k in range(0, e2e_steps, batch):
             cams = L.cams(f + k, batch)
             L.launch(cams, L.cams(f + k + batch, batch))
-            for b in range(batch):
-                host8[b].copy_(L.bufs[b][1], non_blocking=True)
+            for i, (b, nb) in enumerate(L.outputs(cams)):
+                host8[i][:nb].copy_(b[:nb], non_blocking=True)
+                d2h += nb
+            e2e_rays += L.rays(cams)
             stream.synchronize()
     e2e_s = time.perf_counter() - t0
     import ctypes
-    e2e = {"value": round(W * H * e2e_frames / e2e_s * world, 1), "unit": "rays/s",
-           "h2d_bytes_per_step": ctypes.sizeof(wl.vt.vt_camera), "d2h_bytes_per_step": W * H * 3,
-           "ms_per_step": round(e2e_s * 1e3 / e2e_frames, 3), "steps": e2e_frames,
-           "note": "continues the fly-through after the timed frames; wall clock around the public API "
-                   "(vt_render / vt_render_batch) plus the D2H copy of every RGB8 frame"}
-    # the plain LRU renderer on the same frames, for comparison
+    per_view = ctypes.sizeof(wl.vt.vt_camera)
+    views_per_step = cfg["views"]["n"] if "views" in cfg else 1
+    e2e = {"value": round(e2e_rays / e2e_s * world, 1), "unit": "rays/s",
+           "h2d_bytes_per_step": per_view * views_per_step, "d2h_bytes_per_step": int(d2h / e2e_steps),
+           "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3), "steps": e2e_steps,
+           "note": "continues the workload after the timed steps; wall clock around the public API "
+                   "(vt_render / vt_render_batch) plus the D2H copy of every RGB8 image"}
+    # the plain LRU renderer on the same steps, for comparison
     plain = None
     if args.mode != "plain" and not cfg["resident"] and not args.no_plain:
         wl.r.close()
         rp = wl.renderer("plain")
-        Lp = Launcher(wl, rp, cfg, torch, dev, stream, batch=1)
+        Lp = make_launcher(wl, rp, cfg, torch, dev, stream, 1, plain=True)
         pms, pper, _, _ = timed_frames(Lp, frame0, args.warmup, args.steps, dist)
         ps = rp.stats()
         plain = {"value": round(rays_rank * world / (sum(pms) * 1e-3), 1), "unit": "rays/s",
@@ -437,17 +587,25 @@ def run_ours(args, cfg, rank, world, torch, dist):
         rp.close()
     if rank != 0:
         return None
+    W, H = cfg["W"], cfg["H"]
+    if "views" in cfg:
+        conf = {"views_per_launch": cfg["views"]["n"], "resolutions": [list(r) for r in cfg["views"]["res"]],
+                "rays_per_step": round(rays_rank / args.steps)}
+    else:
+        conf = {"W": W, "H": H, "frames_per_launch": batch}
     line = {
-        "metric": "rays/s & ms/frame on 1 B200 (%s)" % ("resident march" if cfg["resident"] else
-                                                         "out-of-core fly-through, %s renderer" % args.mode),
+        "metric": "rays/s & ms/frame on 1 B200 (%s)" % (
+            "resident march" if cfg["resident"] else
+            ("batched views, %s renderer; a step is one batch of views" % args.mode) if "views" in cfg else
+            "out-of-core fly-through, %s renderer" % args.mode),
         "value": round(value, 1), "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, device-generated)",
-        "config": {"workload": cfg["workload"], "name": args.config, "mode": args.mode, "W": W, "H": H,
-                   "frames_per_launch": batch, "learned_prefetch": P is not None,
+        "config": dict(conf, workload=cfg["workload"], name=args.config, mode=args.mode,
+                       learned_prefetch=P is not None, brick=wl.brick, **{
                    "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": roofline(ld, trace_tot, W * H * args.steps),
+                   "parallelism": "replicas" if world > 1 else "single GPU"}),
+        "roofline": roofline(ld, trace_tot, rays_rank),
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": int(st["launches"]),
@@ -468,8 +626,10 @@ def run_ours(args, cfg, rank, world, torch, dist):
         line["learned_prefetch"] = wl.train_info
     if tune:
         line["autotune"] = {"best": tune["best"], "points": tune["points"]}
+        if tune["bricks"]:
+            line["autotune"]["bricks"] = tune["bricks"]
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, frame=frame0 + args.warmup)
+        line["cpu_baseline"] = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, step=frame0 + args.warmup)
     return line
 
 
@@ -479,17 +639,22 @@ def run_reference(args, cfg, rank, world, torch):
     dev = torch.device("cuda", 0)
     work = tempfile.mkdtemp(prefix="vtbench_ref_")
     wl = Workload(cfg, torch, dev, work, need_renderer=False)
-    n = cfg["W"] * cfg["H"]
+    if "views" in cfg:
+        n = sum(c.W * c.H for c in step_views(cfg, args.warmup))
+    else:
+        n = cfg["W"] * cfg["H"]
     vals = []
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(cfg, wl, wl.octree_path, args.ref_budget, frame=i)
+        cb = cpu_baseline(cfg, wl, wl.octree_path, args.ref_budget, step=i)
         if i >= args.warmup:
             vals.append(cb)
     rays_s = statistics.median(v["value"] for v in vals)
     line = {
         "impl": "reference",
-        "metric": "rays/s & ms/frame on 1 B200 (plain LRU renderer, single view)" if cfg["orbit"] else
-                  "rays/s & ms/frame on 1 B200 (resident march)",
+        "metric": "rays/s & ms/frame on 1 B200 (%s)" % (
+            "resident march" if cfg["resident"] else
+            ("batched views, best renderer; a step is one batch of views" if "views" in cfg else
+             "out-of-core fly-through, best renderer")),
         "value": rays_s, "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(n / rays_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
@@ -516,6 +681,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-LRU comparison run")
     ap.add_argument("--no-learned", action="store_true", help="best mode without the learned prefetch")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-brick-sweep", action="store_true", help="batched configs: keep the config's brick size")
     ap.add_argument("--warm", action="store_true", help="profiling: preloaded cache, no cold start")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -532,7 +698,7 @@ def main():
         dist = tdist
     cfg = CONFIGS[args.config]
     if args.steps is None:
-        args.steps = 300 if cfg["orbit"] else 200     # c2: the 300-frame orbit
+        args.steps = 300 if cfg["orbit"] else (6 if "views" in cfg else 200)   # c2: the 300-frame orbit
     if args.impl == "reference":
         line = run_reference(args, cfg, rank, world, torch)
     else:

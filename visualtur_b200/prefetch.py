@@ -113,10 +113,17 @@ class Prefetcher:
     def __init__(self, n, fov, levelC, brick_list, seed=0, hidden=512, level=TRACE_LEVEL):
         self.n, self.fov, self.levelC, self.level = n, fov, levelC, level
         self.mlp = MLP((FEATURES, hidden, hidden, 8 ** level), seed=seed)
-        self.groups = node_bricks(brick_list, levelC, level)
+        self.set_bricks(brick_list, levelC)
+
+    def set_bricks(self, brick_list, levelC):
+        """Brick codes (at levelC) that hints are drawn from: a renderer with
+        another brick size takes its own list; the network is unchanged."""
+        self.levelC = levelC
+        self.groups = node_bricks(brick_list, levelC, self.level)
         # bricks with the coarse node each lies in, for vectorised selection
         self.bricks = np.sort(np.asarray(brick_list, np.uint64))
-        self.brick_node = ((self.bricks >> np.uint64(3 * (levelC - level))) - np.uint64(8 ** level)).astype(np.int64)
+        self.brick_node = ((self.bricks >> np.uint64(3 * (levelC - self.level))) -
+                           np.uint64(8 ** self.level)).astype(np.int64)
 
     def train(self, torch, X, Y, epochs=30, batch=256, lr=1e-3, seed=0):
         """X: N x 12 features, Y: N x 8^level targets; returns per-epoch loss"""
