@@ -420,7 +420,7 @@ class ViewLauncher:
             self.r.render_batch(views, stream=sp)
 
 
-def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
+def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, label="timed"):
     """Renders `warmup` then `steps` consecutive frames in launches of
     L.batch; returns device ms (CUDA events on the launching stream) and
     stats per launch, and the number of frames in each."""
@@ -451,6 +451,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
         torch.cuda.synchronize()
         if clocks:
             clocks.start()
+        torch.cuda.nvtx.range_push(label)     # the timed region, for launch lists (ncu --nvtx-include)
         for k, (f0, n, cams, nxt) in enumerate(launches):
             if flush is not None:
                 flush.zero_()
@@ -459,6 +460,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False):
             ev[k][1].record(stream)
             per.append(r.stats())
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         if dist:
             dist.barrier()
     clk = clocks.stop() if clocks else None
@@ -576,7 +578,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
         wl.r.close()
         rp = wl.renderer("plain")
         Lp = make_launcher(wl, rp, cfg, torch, dev, stream, 1, plain=True)
-        pms, pper, _, _ = timed_frames(Lp, frame0, args.warmup, args.steps, dist)
+        pms, pper, _, _ = timed_frames(Lp, frame0, args.warmup, args.steps, dist, label="plain")
         ps = rp.stats()
         plain = {"value": round(rays_rank * world / (sum(pms) * 1e-3), 1), "unit": "rays/s",
                  "ms_per_step": round(sum(pms) / args.steps, 4),

@@ -79,6 +79,11 @@ CASES = {
     # the 128^3 noisy-sphere volume of the resident benchmark, 8^3 bricks
     "c1": dict(seed=1234, n=128, c=(63.5, 63.5, 63.5), sigma=0.25, iso=40.0, levelC=4, levelO=5, inc=3,
                W=128, H=128, fov=30.0, dist=50.0, ops=[("mv", (63.5, 63.5, 363.5))]),
+    # camera on node planes (x = y = 64) with an odd screen: slab products of
+    # exactly 0, coincident events and infinite reciprocals exercise the
+    # traversal's exact-tie paths
+    "c1plane": dict(seed=1234, n=128, c=(63.5, 63.5, 63.5), sigma=0.25, iso=40.0, levelC=4, levelO=5, inc=3,
+                    W=65, H=65, fov=20.0, dist=50.0, ops=[("mv", (64.0, 64.0, 200.0))]),
     # camera inside the volume's bounding box (tnear clamped to 0 paths)
     "c1in": dict(seed=1234, n=128, c=(63.5, 63.5, 63.5), sigma=0.25, iso=40.0, levelC=4, levelO=5, inc=3,
                  W=64, H=64, fov=40.0, dist=50.0, ops=[("mv", (63.5, 70.25, 120.0)), ("ry", 17.0)]),

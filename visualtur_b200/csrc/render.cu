@@ -60,10 +60,19 @@ __device__ __forceinline__ float interp(const Samp& s, float3 p) {
 /* getNormal (src/rayCaster.cu:131-137). */
 template <int VTYPE>
 __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
-    float gx = (interp<VTYPE>(s, f3(p.x - 1.0f, p.y, p.z)) - interp<VTYPE>(s, f3(p.x + 1.0f, p.y, p.z))) / 2.0f;
-    float gy = (interp<VTYPE>(s, f3(p.x, p.y - 1.0f, p.z)) - interp<VTYPE>(s, f3(p.x, p.y + 1.0f, p.z))) / 2.0f;
-    float gz = (interp<VTYPE>(s, f3(p.x, p.y, p.z - 1.0f)) - interp<VTYPE>(s, f3(p.x, p.y, p.z + 1.0f))) / 2.0f;
-    return normalize(f3(gx, gy, gz));
+    /* six taps through one call site: shading runs once per hit ray, and
+     * the smaller kernel keeps the traversal loop in the instruction cache */
+    float v[6];
+#pragma unroll 1
+    for (int t = 0; t < 6; t++) {
+        const float d = (t & 1) ? 1.0f : -1.0f;
+        float3 q = p;
+        if (t < 2) q.x = p.x + d;
+        else if (t < 4) q.y = p.y + d;
+        else q.z = p.z + d;
+        v[t] = interp<VTYPE>(s, q);
+    }
+    return normalize(f3((v[0] - v[1]) / 2.0f, (v[2] - v[3]) / 2.0f, (v[4] - v[5]) / 2.0f));
 }
 
 /* The march of cuda_rayCaster (src/rayCaster.cu:166-237): samples at
@@ -221,8 +230,74 @@ __device__ __forceinline__ bool expand(const TraceArgs& A, const RayInv& r, Stk&
                 y2 = ((float)(my + 2 * cd) - r.o.y) * r.dy;
     const float z0 = ((float)mz - r.o.z) * r.dz, z1 = ((float)(mz + cd) - r.o.z) * r.dz,
                 z2 = ((float)(mz + 2 * cd) - r.o.z) * r.dz;
+    /* entry / exit parameter of the low (0) and high (1) half on each axis,
+     * ordered by the direction's sign as the reference's slab test orders
+     * them (src/Octree.cu:268-300) */
     const bool sx = r.dx >= 0, sy = r.dy >= 0, sz = r.dz >= 0;
+    const float ex0 = sx ? x0 : x1, fx0 = sx ? x1 : x0, ex1 = sx ? x1 : x2, fx1 = sx ? x2 : x1;
+    const float ey0 = sy ? y0 : y1, fy0 = sy ? y1 : y0, ey1 = sy ? y1 : y2, fy1 = sy ? y2 : y1;
+    const float ez0 = sz ? z0 : z1, fz0 = sz ? z1 : z0, ez1 = sz ? z1 : z2, fz1 = sz ? z2 : z1;
     const unsigned int m = nd.y;
+    /* Fast path (parametric traversal).  Inside the node the ray's
+     * parameter runs from T0 to T1 and changes half on axis a where it
+     * crosses the mid-plane, at t = a1.  When T0, T1, the three crossings
+     * and 0 are finite and pairwise distinct, the children the slab tests
+     * accept are exactly the segments between consecutive events whose end
+     * is >= 0; their tnear values are the segment starts, distinct after
+     * the clamp to 0, so (tnear, tfar) order is segment order.  The
+     * segments, filtered by membership, are pushed directly; any
+     * coincidence, infinity or NaN takes the literal path below. */
+    if (sortChildren) {
+        const float T0 = fmaxf(fmaxf(sx ? x0 : x2, sy ? y0 : y2), sz ? z0 : z2);
+        const float T1 = fminf(fminf(sx ? x2 : x0, sy ? y2 : y0), sz ? z2 : z0);
+        bool ok = isfinite(x0) && isfinite(x1) && isfinite(x2) && isfinite(y0) && isfinite(y1) && isfinite(y2) &&
+                  isfinite(z0) && isfinite(z1) && isfinite(z2) && T0 < T1;
+        ok = ok && T0 != x1 && T0 != y1 && T0 != z1 && T0 != 0.0f && T1 != x1 && T1 != y1 && T1 != z1 &&
+             T1 != 0.0f && x1 != y1 && x1 != z1 && y1 != z1 && x1 != 0.0f && y1 != 0.0f && z1 != 0.0f;
+        if (ok) {
+            /* half of each axis at entry: the sign-ordered first half while
+             * the crossing lies ahead */
+            const int kx = (x1 > T0) ? (sx ? 0 : 1) : (sx ? 1 : 0);
+            const int ky = (y1 > T0) ? (sy ? 0 : 1) : (sy ? 1 : 0);
+            const int kz = (z1 > T0) ? (sz ? 0 : 1) : (sz ? 1 : 0);
+            /* crossings inside (T0, T1), sorted with the child-index bit each flips */
+            const float INF = __int_as_float(0x7f800000);
+            float c0 = (x1 > T0 && x1 < T1) ? x1 : INF, c1 = (y1 > T0 && y1 < T1) ? y1 : INF,
+                  c2 = (z1 > T0 && z1 < T1) ? z1 : INF;
+            int b0 = 4, b1 = 2, b2 = 1;
+            if (c1 < c0) { float t = c0; c0 = c1; c1 = t; int b = b0; b0 = b1; b1 = b; }
+            if (c2 < c1) { float t = c1; c1 = c2; c2 = t; int b = b1; b1 = b2; b2 = b; }
+            if (c1 < c0) { float t = c0; c0 = c1; c1 = t; int b = b0; b0 = b1; b1 = b; }
+            const int n1 = c0 < INF, n2 = c1 < INF, n3 = c2 < INF;
+            const int ch0 = (kx << 2) | (ky << 1) | kz, ch1 = ch0 ^ b0, ch2 = ch1 ^ b1, ch3 = ch2 ^ b2;
+            const bool a0 = (n1 ? c0 : T1) >= 0.0f && ((m >> ch0) & 1u);
+            const bool a1 = n1 && (n2 ? c1 : T1) >= 0.0f && ((m >> ch1) & 1u);
+            const bool a2 = n2 && (n3 ? c2 : T1) >= 0.0f && ((m >> ch2) & 1u);
+            const bool a3 = n3 && T1 >= 0.0f && ((m >> ch3) & 1u);
+            const int nvf = (int)a0 + (int)a1 + (int)a2 + (int)a3;
+            if (top + nvf >= VT_STACK) {
+                atomicOr(A.ctl.err, VT_KERR_STACK);
+                top = -1;
+                return false;
+            }
+            /* near to far: the first accepted segment ends on top */
+            int q = top + nvf;
+            const int chs[4] = {ch0, ch1, ch2, ch3};
+            const bool acc[4] = {a0, a1, a2, a3};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                if (acc[i]) {
+                    const int k = chs[i];
+                    const unsigned int cidx = cl < Lo ? nd.x + __popc(m & ((1u << k) - 1u)) : 0u;
+                    st.e[q--] = make_entry(cidx, cl, (px_ << 1) | ((k >> 2) & 1), (py_ << 1) | ((k >> 1) & 1),
+                                           (pz_ << 1) | (k & 1));
+                }
+            }
+            top += nvf;
+            if ((unsigned int)(top + 1) > cnt[VT_C_MAXSTACK]) cnt[VT_C_MAXSTACK] = top + 1;
+            return true;
+        }
+    }
     unsigned long long cent[8];
     float ctn[8], ctf[8];
     int nv = 0;
@@ -230,11 +305,9 @@ __device__ __forceinline__ bool expand(const TraceArgs& A, const RayInv& r, Stk&
     for (int k = 0; k < 8; k++) {
         if ((m >> k) & 1u) {
             const int kx = (k >> 2) & 1, ky = (k >> 1) & 1, kz = k & 1;
-            const float xa = kx ? x1 : x0, xb = kx ? x2 : x1;
-            const float ya = ky ? y1 : y0, yb = ky ? y2 : y1;
-            const float za = kz ? z1 : z0, zb = kz ? z2 : z1;
             float a, b;
-            if (slab_t(sx ? xa : xb, sx ? xb : xa, sy ? ya : yb, sy ? yb : ya, sz ? za : zb, sz ? zb : za, &a, &b) &&
+            if (slab_t(kx ? ex1 : ex0, kx ? fx1 : fx0, ky ? ey1 : ey0, ky ? fy1 : fy0, kz ? ez1 : ez0, kz ? fz1 : fz0,
+                       &a, &b) &&
                 b >= 0.0f) {
                 unsigned int cidx = cl < Lo ? nd.x + __popc(m & ((1u << k) - 1u)) : 0u;
                 cent[nv] = make_entry(cidx, cl, (px_ << 1) | kx, (py_ << 1) | ky, (pz_ << 1) | kz);
@@ -464,9 +537,12 @@ __device__ __forceinline__ void flush_counters(const TraceArgs& A, unsigned int*
 /* One ray per thread (PERSIST = false) or a persistent ray queue: each warp
  * keeps its 32 lanes busy, and after every `pops` traversal steps the lanes
  * whose ray finished or suspended take new work items -- a ballot of the
- * idle lanes, one atomicAdd by the leader, and a popcount rank per lane. */
+ * idle lanes, one atomicAdd by the leader, and a popcount rank per lane.
+ * Eight 128-thread CTAs per SM (64 registers a thread): the traversal is
+ * latency-bound, and the extra resident warps hide more of it than the
+ * few spilled registers cost. */
 template <int VTYPE, bool SLAB, bool PERSIST, int U>
-__global__ void __launch_bounds__(128) k_trace(TraceArgs A) {
+__global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
     __shared__ DevView sv[VT_MAX_VIEWS];
     for (int k = threadIdx.x; k < A.views.n; k += blockDim.x) sv[k] = A.views.v[k];
     __syncthreads();
