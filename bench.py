@@ -351,13 +351,17 @@ class Launcher:
         """(device RGB8 buffer, bytes) of each frame of the last launch"""
         return [(self.bufs[b][1], c.W * c.H * 3) for b, c in enumerate(cams)]
 
+    hint_s = 0.0
+
     def hint(self, cams):
         if self.P is None or not cams:
             return
+        t0 = time.perf_counter()
         from visualtur_b200 import prefetch as pf
         feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for c in cams])
         probs = self.P.predict(self.torch, feats).max(axis=0)
         self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
+        self.hint_s += time.perf_counter() - t0
 
     def launch(self, cams, next_cams=()):
         self.hint(list(cams) + list(next_cams))
@@ -397,13 +401,17 @@ class ViewLauncher:
     def outputs(self, items):
         return [(b, c.W * c.H * 3) for c, b in zip(items[-1], self.bufs)]
 
+    hint_s = 0.0
+
     def hint(self, items):
         if self.P is None or not items:
             return
+        t0 = time.perf_counter()
         from visualtur_b200 import prefetch as pf
         feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for views in items for c in views])
         probs = self.P.predict(self.torch, feats).max(axis=0)
         self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
+        self.hint_s += time.perf_counter() - t0
 
     def launch(self, items, next_items=()):
         self.hint(list(items) + list(next_items))
@@ -451,6 +459,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
         torch.cuda.synchronize()
         if clocks:
             clocks.start()
+        L.hint_s = 0.0
         torch.cuda.nvtx.range_push(label)     # the timed region, for launch lists (ncu --nvtx-include)
         for k, (f0, n, cams, nxt) in enumerate(launches):
             if flush is not None:
@@ -461,6 +470,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
             per.append(r.stats())
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
+        L.timed_hint_s = L.hint_s
         if dist:
             dist.barrier()
     clk = clocks.stop() if clocks else None
@@ -615,6 +625,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
                         "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in per) / args.steps, 4),
                         "prefetch_ms_per_step": round(sum(s["ms_prefetch_last_frame"] for s in per) / args.steps, 4),
                         "trace_ms_per_step": round(trace_tot / args.steps, 4),
+                        "hint_host_ms_per_step": round(getattr(L, "timed_hint_s", 0.0) * 1e3 / args.steps, 4),
+                        "host_ms_per_step": round(sum(s["ms_last_frame"] for s in per) / args.steps, 4),
                         "device_hit_rate": round(st["device_hits"] / max(1, st["device_hits"] + st["device_misses"]), 5),
                         "bricks_requested": st["bricks_requested"], "bricks_loaded": st["bricks_loaded_disk"],
                         "bricks_prefetched": st["bricks_prefetched"], "bricks_hinted": st["bricks_hinted"],

@@ -36,17 +36,28 @@ struct Samp {
 };
 
 /* getElementInterpolate (src/rayCaster.cu:86-106). */
-template <int VTYPE>
+template <int VTYPE, bool SLAB = false>
 __device__ __forceinline__ float interp(const Samp& s, float3 p) {
     float rx, ry, rz;
     float px = modff(p.x, &rx), py = modff(p.y, &ry), pz = modff(p.z, &rz);
     int x0 = f2i(rx - (float)s.ox), y0 = f2i(ry - (float)s.oy), z0 = f2i(rz - (float)s.oz);
     x0 = min(max(x0, 0), s.hx); y0 = min(max(y0, 0), s.hy); z0 = min(max(z0, 0), s.hz);
-    long long b = (long long)x0 * s.sx + (long long)y0 * s.sy + z0;
-    float v000 = ldv<VTYPE>(s.base, b), v001 = ldv<VTYPE>(s.base, b + 1);
-    float v010 = ldv<VTYPE>(s.base, b + s.sy), v011 = ldv<VTYPE>(s.base, b + s.sy + 1);
-    float v100 = ldv<VTYPE>(s.base, b + s.sx), v101 = ldv<VTYPE>(s.base, b + s.sx + 1);
-    float v110 = ldv<VTYPE>(s.base, b + s.sx + s.sy), v111 = ldv<VTYPE>(s.base, b + s.sx + s.sy + 1);
+    float v000, v001, v010, v011, v100, v101, v110, v111;
+    if (SLAB) {
+        /* a brick holds < 2^31 voxels: 32-bit index arithmetic */
+        const int sx = (int)s.sx, sy = (int)s.sy;
+        const int b = x0 * sx + y0 * sy + z0;
+        v000 = ldv<VTYPE>(s.base, b); v001 = ldv<VTYPE>(s.base, b + 1);
+        v010 = ldv<VTYPE>(s.base, b + sy); v011 = ldv<VTYPE>(s.base, b + sy + 1);
+        v100 = ldv<VTYPE>(s.base, b + sx); v101 = ldv<VTYPE>(s.base, b + sx + 1);
+        v110 = ldv<VTYPE>(s.base, b + sx + sy); v111 = ldv<VTYPE>(s.base, b + sx + sy + 1);
+    } else {
+        const long long b = (long long)x0 * s.sx + (long long)y0 * s.sy + z0;
+        v000 = ldv<VTYPE>(s.base, b); v001 = ldv<VTYPE>(s.base, b + 1);
+        v010 = ldv<VTYPE>(s.base, b + s.sy); v011 = ldv<VTYPE>(s.base, b + s.sy + 1);
+        v100 = ldv<VTYPE>(s.base, b + s.sx); v101 = ldv<VTYPE>(s.base, b + s.sx + 1);
+        v110 = ldv<VTYPE>(s.base, b + s.sx + s.sy); v111 = ldv<VTYPE>(s.base, b + s.sx + s.sy + 1);
+    }
     float qx = 1.0f - px, qy = 1.0f - py, qz = 1.0f - pz;
     float c00 = v000 * qx + v100 * px;
     float c01 = v001 * qx + v101 * px;
@@ -58,7 +69,7 @@ __device__ __forceinline__ float interp(const Samp& s, float3 p) {
 }
 
 /* getNormal (src/rayCaster.cu:131-137). */
-template <int VTYPE>
+template <int VTYPE, bool SLAB>
 __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
     /* six taps through one call site: shading runs once per hit ray, and
      * the smaller kernel keeps the traversal loop in the instruction cache */
@@ -70,7 +81,7 @@ __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
         if (t < 2) q.x = p.x + d;
         else if (t < 4) q.y = p.y + d;
         else q.z = p.z + d;
-        v[t] = interp<VTYPE>(s, q);
+        v[t] = interp<VTYPE, SLAB>(s, q);
     }
     return normalize(f3((v[0] - v[1]) / 2.0f, (v[2] - v[3]) / 2.0f, (v[4] - v[5]) / 2.0f));
 }
@@ -88,14 +99,14 @@ __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
  * iso - value has the same strict sign as its own (the crossing test's
  * "no crossing" condition), so the pair keeps bracketing the crossing.
  * Each midpoint is one more trilinear sample. */
-template <int VTYPE, int U>
+template <int VTYPE, bool SLAB, int U>
 __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, float tnear,
                                       int maxStep, float iso, int refine, float3* Xhit, unsigned int* nsamp) {
     float3 Xnear = add(origin, mul(ray, tnear));
     float3 Xfar = Xnear;
     float3 vStep = mul(ray, 0.5f);
     if (maxStep < 0) return false;
-    float ant = interp<VTYPE>(s, Xnear);
+    float ant = interp<VTYPE, SLAB>(s, Xnear);
     unsigned int ns = 1;
     bool hit = false;
     for (int steps = 1; steps <= maxStep && !hit; steps += U) {
@@ -104,7 +115,7 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
 #pragma unroll
         for (int u = 0; u < U; u++) X[u] = add(u == 0 ? Xnear : X[u - 1], vStep);
 #pragma unroll
-        for (int u = 0; u < U; u++) v[u] = interp<VTYPE>(s, X[u]);
+        for (int u = 0; u < U; u++) v[u] = interp<VTYPE, SLAB>(s, X[u]);
 #pragma unroll
         for (int u = 0; u < U; u++) {
             if (hit || steps + u > maxStep) break;
@@ -118,7 +129,7 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
                 float3 P = Xfar, Q = X[u];
                 for (int k = 0; k < refine; k++) {
                     float3 M = mul(add(P, Q), 0.5f);
-                    float vm = interp<VTYPE>(s, M);
+                    float vm = interp<VTYPE, SLAB>(s, M);
                     ns++;
                     if ((((iso - ant) < 0.0f) && ((iso - vm) < 0.0f)) ||
                         (((iso - ant) > 0.0f) && ((iso - vm) > 0.0f))) {
@@ -184,6 +195,7 @@ __device__ __forceinline__ void setup_sampler(const TraceArgs& A, unsigned int b
 /* One ray in flight. */
 struct Ray {
     RayInv r;
+    int lastSlot;          /* slot whose stamp this ray wrote last */
     float3 dir;
     int top;
     int view, i, j;
@@ -384,7 +396,10 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
         }
         R.top--;
         cnt[VT_C_CANDIDATES]++;
-        if (SLAB) { cnt[VT_C_DEVHITS]++; A.br.stamp[slot] = A.br.pass; }
+        if (SLAB) {
+            cnt[VT_C_DEVHITS]++;
+            if (slot != R.lastSlot) { A.br.stamp[slot] = A.br.pass; R.lastSlot = slot; }   /* once per brick run */
+        }
         if (A.ctl.touched) {
             const int d = A.ctl.touch_shift / 3;   /* Lo - trace level */
             unsigned long long tn = (spread3(x >> d) << 2) | (spread3(y >> d) << 1) | spread3(z >> d);
@@ -395,11 +410,11 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
         if (!slab(R.r, mbx, mby, mbz, mbx + dimO, mby + dimO, mbz + dimO, &tn, &tf)) continue;
         float3 X;
         unsigned int ns = 0;
-        bool h = march<VTYPE, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
+        bool h = march<VTYPE, SLAB, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
         cnt[VT_C_SAMPLES] += ns;
         if (h) {
             /* shade (src/rayCaster.cu:238-250) */
-            float3 n = normal_at<VTYPE>(s, X);
+            float3 n = normal_at<VTYPE, SLAB>(s, X);
             cnt[VT_C_NSAMPLES] += 6;
             float3 l = normalize(sub(X, A.light));
             float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
@@ -470,6 +485,7 @@ __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, 
     R.rgba = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     R.hit = false; R.node = 0; R.brick = 0; R.t = -1.0f; R.n = f3(0, 0, 0);
     R.top = -1;
+    R.lastSlot = -1;
     if (resume && depth > 0) {
         R.top = (int)depth - 1;
         for (int e = 0; e <= R.top; e++) st.e[e] = A.ctl.pool_in[off + e];
