@@ -43,6 +43,12 @@ sys.path.insert(0, ROOT)
 
 HBM_FALLBACK_GBS = 6650.0
 
+# DRAM bytes per ray of k_trace (dram__bytes_read.sum + dram__bytes_write.sum
+# of one ncu capture of a full 1920x1080 frame of the c2s fly-through, warm
+# cache; the c2 orbit is the same view of a volume twice the size, with the
+# same samples per ray).  Scaled by the rays of a launch for roofline.traffic.
+TRAFFIC_BYTES_PER_RAY = {"c2": 94.6, "c2s": 94.6}
+
 CONFIGS = {
     "c1": dict(workload="128^3 f32 noisy sphere (|x-c|+N(0,0.25)), iso 40, resident, 512x512, FOV 60 deg, "
                         "distance 300, 8^3 bricks, 4^3 candidate nodes",
@@ -266,7 +272,7 @@ class Workload:
         return P
 
 
-def roofline(stats_frames, trace_ms, pixels):
+def roofline(stats_frames, trace_ms, pixels, traffic_per_ray=None):
     """Algorithmic bytes of the march (4 B voxels, 8 taps per sample, 6 extra
     samples per hit for the normal) + 4 B per output pixel, over the trace
     kernels' device time."""
@@ -281,7 +287,9 @@ def roofline(stats_frames, trace_ms, pixels):
         pass
     ach = b_alg / (trace_ms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "peak_source": src, "unit": "GB/s",
-            "frac": round(ach / peak, 4), "traffic": None, "bytes_alg_per_launch": b_alg / len(stats_frames),
+            "frac": round(ach / peak, 4),
+            "traffic": round(traffic_per_ray * pixels / len(stats_frames)) if traffic_per_ray else None,
+            "bytes_alg_per_launch": b_alg / len(stats_frames),
             "kernel": "k_trace"}
 
 
@@ -617,7 +625,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
                        learned_prefetch=P is not None, brick=wl.brick, **{
                    "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
                    "parallelism": "replicas" if world > 1 else "single GPU"}),
-        "roofline": roofline(ld, trace_tot, rays_rank),
+        "roofline": roofline(ld, trace_tot, rays_rank, TRAFFIC_BYTES_PER_RAY.get(args.config)),
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": int(st["launches"]),
