@@ -77,6 +77,19 @@ CONFIGS = {
                 blobs=(256, 10.0, 60.0, 0.5, 1.5, 0.05),
                 views=dict(n=64, r=(1250.0, 1750.0), res=((256, 256), (512, 512), (1024, 1024), (1920, 1080),
                                                           (2048, 2048)))),
+    # 4096^3 uint8 fractal with spheres, 32^3 bricks, 600-frame spline
+    "c5": dict(workload="4096^3 u8 6-octave fractal value noise + 32 spheres (value 200, radius 50-400), iso 128, "
+                        "out-of-core: 32^3 bricks (apron 3), 16 GB device cache, 64 GB pinned host tier, 1920x1080, "
+                        "600-frame Catmull-Rom path through 12 seeded control points, timed from a cold cache",
+               gen="fractal", seed=4096, n=4096, iso=128.0, levelC=7, levelO=10, inc=3, W=1920, H=1080, fov=30.0,
+               dist=50.0, resident=0, l2flush=False, orbit=None, dev_bytes=16 << 30, host_bytes=64 << 30,
+               spheres=(32, 50.0, 400.0, 200.0), path=dict(frames=600, ctrl=12, r=(3500.0, 5000.0))),
+    # c5 scaled by 1/2 per axis (8 GB volume)
+    "c5s": dict(workload="2048^3 u8 fractal + 32 spheres (c5 scaled by 1/2), iso 128, 32^3 bricks, 2 GB device "
+                         "cache, 8 GB host tier, 1920x1080, 600-frame spline",
+                gen="fractal", seed=4096, n=2048, iso=128.0, levelC=6, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
+                dist=50.0, resident=0, l2flush=False, orbit=None, dev_bytes=2 << 30, host_bytes=8 << 30,
+                spheres=(32, 25.0, 200.0, 200.0), path=dict(frames=600, ctrl=12, r=(1750.0, 2500.0))),
     # profiling-sized version of c2 (1 GB volume) for ncu captures
     "c2s": dict(workload="1024^3 f32 blobs+noise (c2 scaled by 1/2), iso 0.6, 16^3 bricks, 1920x1080, orbit r=1500",
                 gen="blobs", seed=2048, n=1024, iso=0.6, levelC=6, levelO=8, inc=3, W=1920, H=1080, fov=30.0,
@@ -160,7 +173,27 @@ def static_camera(vt, cfg):
     return cam.c
 
 
+_PATHS = {}
+
+
+def path_camera(cfg, frame):
+    """Pose `frame` of a seeded Catmull-Rom fly-through: positions through
+    cfg["path"]["ctrl"] control points on a shell around the volume, looking
+    at a spline through targets in the inner half (frames wrap around)."""
+    from visualtur_b200 import prefetch as pf
+    spec, n = cfg["path"], cfg["n"]
+    key = (cfg["seed"], n, spec["frames"])
+    if key not in _PATHS:
+        _PATHS[key] = pf.random_flythrough(np.random.default_rng([cfg["seed"], 5]), n, spec["frames"],
+                                           spec["r"][0], spec["r"][1], ctrl=spec["ctrl"])
+    pos, tgt = _PATHS[key]
+    f = frame % spec["frames"]
+    return pf.look_at(cfg["W"], cfg["H"], cfg["dist"], cfg["fov"], pos[f], tgt[f])
+
+
 def frame_camera(vt, cfg, frame):
+    if cfg.get("path"):
+        return path_camera(cfg, frame)
     return orbit_camera(vt, cfg, frame) if cfg["orbit"] else static_camera(vt, cfg)
 
 
@@ -189,20 +222,26 @@ class Workload:
         import visualtur_b200 as vt
         self.vt, self.cfg = vt, cfg
         n = cfg["n"]
+        u8 = cfg["gen"] == "fractal"
+        self.esize = 1 if u8 else 4
+        vdt = torch.uint8 if u8 else torch.float32
         t0 = time.time()
-        dvol = torch.empty(n * n * n, dtype=torch.float32, device=device)
+        dvol = torch.empty(n * n * n, dtype=vdt, device=device)
         if cfg["gen"] == "sphere":
             c = (n - 1) / 2.0
             vt.generate_volume(vt.VT_GEN_SPHERE, cfg["seed"], (n, n, n), (c, c, c, 0.25), device_ptr=dvol.data_ptr())
+        elif u8:
+            vt.generate_volume(vt.VT_GEN_FRACTAL_U8, cfg["seed"], (n, n, n), cfg["spheres"], device_ptr=dvol.data_ptr())
         else:
             vt.generate_volume(vt.VT_GEN_BLOBS, cfg["seed"], (n, n, n), cfg["blobs"], device_ptr=dvol.data_ptr())
         torch.cuda.synchronize()
         t1 = time.time()
         self.octree_path = os.path.join(workdir, "vol_%s.oct" % cfg["gen"])
-        vt.build_octree_device(dvol.data_ptr(), vt.VT_F32, (n, n, n), cfg["iso"], self.octree_path)
+        vt.build_octree_device(dvol.data_ptr(), vt.VT_U8 if u8 else vt.VT_F32, (n, n, n), cfg["iso"],
+                               self.octree_path)
         t2 = time.time()
         # host copy of the volume: the out-of-core source and the CPU baseline's input
-        self.host = torch.empty(n * n * n, dtype=torch.float32)
+        self.host = torch.empty(n * n * n, dtype=vdt)
         self.host.copy_(dvol)
         torch.cuda.synchronize()
         del dvol
@@ -227,7 +266,7 @@ class Workload:
         edge = brick or self.brick
         levelC = self.oc.nLevels - int(round(math.log2(edge)))
         D = edge + 2 * cfg["inc"]
-        slot = (D ** 3 * 4 + 15) // 16 * 16
+        slot = (D ** 3 * self.esize + 15) // 16 * 16
         dev = cfg.get("dev_bytes", 0) // slot or 8 ** levelC
         host = cfg.get("host_bytes", 0) // slot or 8 ** levelC
         self.slots = (dev, host, slot)
@@ -256,7 +295,8 @@ class Workload:
                                                 record_hits=0), volume=self.fm, octree=self.oc)
         scale = n / 2048.0
         X, Y = pf.collect_traces(tr, n, W, H, cfg["fov"], np.random.default_rng(7), paths, poses // paths,
-                                 2500 * scale, 3500 * scale, dist=cfg["dist"])
+                                 *(cfg["path"]["r"] if cfg.get("path") else (2500 * scale, 3500 * scale)),
+                                 dist=cfg["dist"])
         bricks = tr.brick_list()
         tr.close()
         torch.cuda.empty_cache()
@@ -272,13 +312,13 @@ class Workload:
         return P
 
 
-def roofline(stats_frames, trace_ms, pixels, traffic_per_ray=None):
+def roofline(stats_frames, trace_ms, pixels, traffic_per_ray=None, esize=4):
     """Algorithmic bytes of the march (4 B voxels, 8 taps per sample, 6 extra
     samples per hit for the normal) + 4 B per output pixel, over the trace
     kernels' device time."""
     samples = sum(s["samples"] for s in stats_frames)
     hits = sum(s["hits"] for s in stats_frames)
-    b_alg = 4 * 8 * (samples + 6 * hits) + 4 * pixels
+    b_alg = esize * 8 * (samples + 6 * hits) + 4 * pixels
     peak, src = HBM_FALLBACK_GBS, "fallback"
     try:
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -360,19 +400,35 @@ class Launcher:
         return [(self.bufs[b][1], c.W * c.H * 3) for b, c in enumerate(cams)]
 
     hint_s = 0.0
+    WINDOW = 16      # frames of the scripted path predicted per network call
 
-    def hint(self, cams):
-        if self.P is None or not cams:
+    @staticmethod
+    def _key(c):
+        return tuple(c.position[:]) + tuple(c.look[:]) + tuple(c.up[:])
+
+    def hint(self, cams, f=None):
+        """Predicted bricks of `cams` (frames f, f+1, ...) as the renderer's
+        hint; the network runs once per WINDOW frames of the path."""
+        if self.P is None or not cams or self.thr is None:
             return
         t0 = time.perf_counter()
         from visualtur_b200 import prefetch as pf
-        feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for c in cams])
-        probs = self.P.predict(self.torch, feats).max(axis=0)
+        cache = self.__dict__.setdefault("_probs", {})
+        if any(self._key(c) not in cache for c in cams):
+            win = self.cams(f, max(self.WINDOW, len(cams))) if f is not None else list(cams)
+            win += [c for c in cams if self._key(c) not in {self._key(w) for w in win}]
+            if len(cache) > 4096:
+                cache.clear()
+            probs = self.P.predict(self.torch, np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"])
+                                                         for c in win]))
+            for c, p in zip(win, probs):
+                cache[self._key(c)] = p
+        probs = np.max(np.stack([cache[self._key(c)] for c in cams]), axis=0)
         self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
         self.hint_s += time.perf_counter() - t0
 
-    def launch(self, cams, next_cams=()):
-        self.hint(list(cams) + list(next_cams))
+    def launch(self, cams, next_cams=(), f=None):
+        self.hint(list(cams) + list(next_cams), f)
         sp = self.stream.cuda_stream
         if self.batch == 1:
             self.r.set_camera(cams[0])
@@ -421,7 +477,7 @@ class ViewLauncher:
         self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
         self.hint_s += time.perf_counter() - t0
 
-    def launch(self, items, next_items=()):
+    def launch(self, items, next_items=(), f=None):
         self.hint(list(items) + list(next_items))
         sp = self.stream.cuda_stream
         views = []
@@ -447,7 +503,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
         while f < frame0 + warmup:
             n = min(L.batch, frame0 + warmup - f)
             nxt = min(L.batch, frame0 + warmup + steps - f - n)
-            L.launch(L.cams(f, n), L.cams(f + n, nxt))
+            L.launch(L.cams(f, n), L.cams(f + n, nxt), f)
             f += n
         torch.cuda.synchronize()
         if not L.cfg["resident"] and not L.warm:
@@ -473,7 +529,7 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
             if flush is not None:
                 flush.zero_()
             ev[k][0].record(stream)
-            L.launch(cams, nxt)
+            L.launch(cams, nxt, f0)
             ev[k][1].record(stream)
             per.append(r.stats())
         torch.cuda.synchronize()
@@ -497,6 +553,46 @@ def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=Fa
     if "views" in cfg:
         return ViewLauncher(wl, r, cfg, torch, dev, stream, predictor=predictor, warm=warm, plain=plain)
     return Launcher(wl, r, cfg, torch, dev, stream, batch=batch, predictor=predictor, warm=warm)
+
+
+PAGING_CANDIDATES = ((8, 2), (4, 2), (2, 2), (1, 2), (1, 0))   # (frames per launch, lookahead)
+HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
+
+
+def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=48):
+    """Frames per launch, lookahead and the prefetch-hint threshold for an
+    out-of-core fly-through: each candidate renders the same `frames`
+    frames (another stretch of the path than the timed one) from a cold
+    cache; the fastest total device time wins.  Batching more frames per
+    launch amortises launches and host work but needs their joint working
+    set in the device cache, and hints help only while the cache has room
+    for them -- a small cache thrashes, which only a cold-cache run shows."""
+    def run(b, la, thr):
+        wl.r.set_tuning(lookahead=la)
+        L = make_launcher(wl, wl.r, cfg, torch, dev, stream, b, predictor=P)
+        L.thr = thr
+        wl.r.drop_cache()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            torch.cuda.synchronize()
+            a.record(stream)
+            for f in range(f0, f0 + frames, b):
+                L.launch(L.cams(f, b), L.cams(f + b, b), f)
+            e.record(stream)
+            torch.cuda.synchronize()
+        ms = a.elapsed_time(e)
+        log("autotune: %d frames/launch, lookahead %d, hints %s -> %.1f ms for %d frames" % (b, la, thr, ms, frames))
+        return {"frames_per_launch": b, "lookahead": la, "hint_threshold": thr, "ms": round(ms, 2)}
+
+    thr0 = 0.5 if P is not None else None
+    rows = [run(b, la, thr0) for b, la in PAGING_CANDIDATES]
+    best = min(rows, key=lambda x: x["ms"])
+    if P is not None:
+        rows += [run(best["frames_per_launch"], best["lookahead"], t) for t in HINT_THRESHOLDS]
+        best = min(rows, key=lambda x: x["ms"])
+    wl.r.set_tuning(lookahead=best["lookahead"])
+    wl.r.drop_cache()
+    return best, rows
 
 
 def autotune(args, wl, cfg, torch, dev, stream, frame0, batch):
@@ -546,11 +642,26 @@ def run_ours(args, cfg, rank, world, torch, dist):
     batch = 1 if (cfg["resident"] or "views" in cfg) else M["batch"]
     P = wl.train_prefetcher(torch) if (M["learned"] and not cfg["resident"] and not args.no_learned) else None
     tune = None
+    paging = None
+    if args.paging and not cfg["resident"] and "views" not in cfg:
+        v = args.paging.split(",")
+        fixed = {"frames_per_launch": int(v[0]), "lookahead": int(v[1]),
+                 "hint_threshold": float(v[2]) if len(v) > 2 and v[2] not in ("", "none") else None}
+        wl.r.set_tuning(lookahead=fixed["lookahead"])
+        batch = fixed["frames_per_launch"]
+        paging = {"best": fixed, "table": []}
+    elif M["autotune"] and not args.no_autotune and not cfg["resident"] and "views" not in cfg:
+        # a stretch of the fly-through away from the timed frames
+        paging, prow = tune_paging(wl, cfg, torch, dev, stream, P, frame0 + args.warmup + args.steps + 97)
+        batch = paging["frames_per_launch"]
+        paging = {"best": paging, "table": prow}
     if M["autotune"] and not args.no_autotune:
         tune = autotune(args, wl, cfg, torch, dev, stream, frame0, batch)
     if P is not None:
         P.set_bricks(wl.r.brick_list(), wl.oc.nLevels - int(round(math.log2(wl.brick))))
     L = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch, predictor=P, warm=args.warm)
+    if paging and P is not None:
+        L.thr = paging["best"]["hint_threshold"]
     ms, per, launches, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index),
                                           cfg["l2flush"])
     tot_ms = sum(ms)
@@ -575,7 +686,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     with torch.cuda.stream(stream):
         for k in range(0, e2e_steps, batch):
             cams = L.cams(f + k, batch)
-            L.launch(cams, L.cams(f + k + batch, batch))
+            L.launch(cams, L.cams(f + k + batch, batch), f + k)
             for i, (b, nb) in enumerate(L.outputs(cams)):
                 host8[i][:nb].copy_(b[:nb], non_blocking=True)
                 d2h += nb
@@ -613,6 +724,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
                 "rays_per_step": round(rays_rank / args.steps)}
     else:
         conf = {"W": W, "H": H, "frames_per_launch": batch}
+        if P is not None and "views" not in cfg:
+            conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
         "metric": "rays/s & ms/frame on 1 B200 (%s)" % (
             "resident march" if cfg["resident"] else
@@ -620,12 +733,13 @@ def run_ours(args, cfg, rank, world, torch, dist):
             "out-of-core fly-through, %s renderer" % args.mode),
         "value": round(value, 1), "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, device-generated)",
+        "vs_baseline": None, "dtype": "u8" if wl.esize == 1 else "f32",
+        "data": "synthetic (seeded generators, device-generated)",
         "config": dict(conf, workload=cfg["workload"], name=args.config, mode=args.mode,
                        learned_prefetch=P is not None, brick=wl.brick, **{
                    "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
                    "parallelism": "replicas" if world > 1 else "single GPU"}),
-        "roofline": roofline(ld, trace_tot, rays_rank, TRAFFIC_BYTES_PER_RAY.get(args.config)),
+        "roofline": roofline(ld, trace_tot, rays_rank, TRAFFIC_BYTES_PER_RAY.get(args.config), wl.esize),
         "e2e": e2e,
         "clocks": clk,
         "gpu_launches": int(st["launches"]),
@@ -648,6 +762,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
         line["learned_prefetch"] = wl.train_info
     if tune:
         line["autotune"] = {"best": tune["best"], "points": tune["points"]}
+        if paging:
+            line["autotune"]["paging"] = paging
         if tune["bricks"]:
             line["autotune"]["bricks"] = tune["bricks"]
     if not args.no_cpu_baseline:
@@ -679,7 +795,7 @@ def run_reference(args, cfg, rank, world, torch):
              "out-of-core fly-through, best renderer")),
         "value": rays_s, "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(n / rays_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "vs_baseline": None, "dtype": "u8" if cfg["gen"] == "fractal" else "f32", "data": "synthetic (seeded generators)",
         "config": {"workload": cfg["workload"], "name": args.config, "W": cfg["W"], "H": cfg["H"]},
         "cpu_baseline": dict(vals[-1], value=rays_s),
         "e2e": {"value": rays_s, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -704,6 +820,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="best mode without the learned prefetch")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-brick-sweep", action="store_true", help="batched configs: keep the config's brick size")
+    ap.add_argument("--paging", default=None, help="fly-throughs: fixed FRAMES,LOOKAHEAD[,HINT_THRESHOLD] instead of "
+                                                   "the paging autotune")
     ap.add_argument("--warm", action="store_true", help="profiling: preloaded cache, no cold start")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -720,7 +838,7 @@ def main():
         dist = tdist
     cfg = CONFIGS[args.config]
     if args.steps is None:
-        args.steps = 300 if cfg["orbit"] else (6 if "views" in cfg else 200)   # c2: the 300-frame orbit
+        args.steps = (300 if cfg["orbit"] else 600 if cfg.get("path") else 6 if "views" in cfg else 200)
     if args.impl == "reference":
         line = run_reference(args, cfg, rank, world, torch)
     else:

@@ -268,6 +268,7 @@ typedef struct {
     int64_t launches;               /* libvt kernels launched (cumulative) */
     int64_t bricks_hinted;          /* bricks named by vt_prefetch and by hints a frame consumed */
     int64_t bricks_staged;          /* of those, absent from the device cache when staged */
+    int64_t bricks_speculative;     /* lookahead requests among bricks_requested */
     double  ms_last_frame, ms_stall_last_frame, bytes_h2d_last_frame;
     double  ms_trace_last_frame;    /* device time of the trace kernels of the last frame */
     double  ms_prefetch_last_frame; /* host time of the hinted prefetch's device fill */

@@ -54,7 +54,7 @@ class vt_stats(C.Structure):
         "frames", "rays", "hits", "samples", "normal_samples", "candidates", "expansions", "passes",
         "bricks_requested", "bricks_loaded_host", "bricks_loaded_disk", "bricks_prefetched",
         "device_hits", "device_misses", "host_hits", "host_misses", "max_stack", "launches",
-        "bricks_hinted", "bricks_staged")] + \
+        "bricks_hinted", "bricks_staged", "bricks_speculative")] + \
         [(n, C.c_double) for n in ("ms_last_frame", "ms_stall_last_frame", "bytes_h2d_last_frame",
                                    "ms_trace_last_frame", "ms_prefetch_last_frame")]
 

@@ -75,11 +75,16 @@ vt_status BrickCache::init(const CacheConfig& c) {
     CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
     CKC(cudaHostAlloc((void**)&h_tier_, slotBytes_ * (size_t)nHost_, cudaHostAllocMapped | cudaHostAllocPortable));
     CKC(cudaHostGetDevicePointer(&d_tier_, h_tier_, 0));
-    slotBrick_.assign(nSlots_, 0);
+    slotBrick_.assign(nSlots_, kEmpty);
+    mark_.assign(nSlots_, 0);
+    freeSlots_.resize(nSlots_);
+    for (int i = 0; i < nSlots_; i++) freeSlots_[i] = nSlots_ - 1 - i;   /* slot 0 is handed out first */
     stampHost_.assign(nSlots_, 0);
     pageMirror_.assign(pageN_, -1);
     hostIndex_.assign(pageN_, -1);
-    hostBrick_.assign(nHost_, 0);
+    hostBrick_.assign(nHost_, kEmpty);
+    freeHost_.resize(nHost_);
+    for (int i = 0; i < nHost_; i++) freeHost_[i] = nHost_ - 1 - i;
     hostTick_.assign(nHost_, 0);
     return VT_OK;
 }
@@ -109,21 +114,22 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
         else miss.push_back(i);
     }
     if (miss.empty()) return VT_OK;
-    /* victims: free host slots first, then least recently used, never a slot
-     * touched in this call */
-    std::vector<int> order(nHost_);
-    std::iota(order.begin(), order.end(), 0);
+    /* victims: never-filled host slots first, then a sweep over the filled
+     * ones skipping every slot touched in this call */
     size_t want = miss.size();
     if (want > (size_t)nHost_) return fail(VT_ERR_STATE, "host tier smaller than one request batch");
-    std::nth_element(order.begin(), order.begin() + (want - 1), order.end(), [&](int a, int b) {
-        bool fa = hostBrick_[a] == 0, fb = hostBrick_[b] == 0;
-        if (fa != fb) return fa;
-        return hostTick_[a] < hostTick_[b];
-    });
+    std::vector<int> order;
+    order.reserve(want);
+    while (order.size() < want && !freeHost_.empty()) { order.push_back(freeHost_.back()); freeHost_.pop_back(); }
+    for (int scanned = 0; scanned < nHost_ && order.size() < want; scanned++) {
+        const int hs = hostClock_;
+        hostClock_ = hostClock_ + 1 == nHost_ ? 0 : hostClock_ + 1;
+        if (hostBrick_[hs] != kEmpty && hostTick_[hs] < callStart) order.push_back(hs);
+    }
+    if (order.size() < want) return fail(VT_ERR_STATE, "host tier exhausted");
     for (size_t k = 0; k < want; k++) {
         int hs = order[k];
-        if (hostBrick_[hs] != 0 && hostTick_[hs] >= callStart) return fail(VT_ERR_STATE, "host tier exhausted");
-        if (hostBrick_[hs] != 0) hostIndex_[hostBrick_[hs] - pageBase_] = -1;
+        if (hostBrick_[hs] != kEmpty) hostIndex_[hostBrick_[hs] - pageBase_] = -1;
         uint64_t b = bricks[miss[k]];
         hostBrick_[hs] = b;
         hostIndex_[b - pageBase_] = hs;
@@ -148,20 +154,29 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
     /* bricks with a host-tier copy, at most one per device slot */
     size_t m = 0;
     while (m < n && m < (size_t)nSlots_ && hslot[m] >= 0) m++;
-    size_t freeCount = 0;
-    for (int i = 0; i < nSlots_; i++) freeCount += slotBrick_[i] == 0;
-    if (freeCount < m) {
+    /* slots: never-filled ones first; then a sweep over the filled slots
+     * with the kernels' stamps, first taking slots not used since the frame
+     * began, then any stamped before protectFrom (slots a kernel of the
+     * current pass used always have a newer stamp) */
+    std::vector<int> order;
+    order.reserve(m);
+    while (order.size() < m && !freeSlots_.empty()) { order.push_back(freeSlots_.back()); freeSlots_.pop_back(); }
+    if (order.size() < m) {
         CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
         CKC(cudaStreamSynchronize(s));
+        ++epoch_;
+        for (int round = 0; round < 2 && order.size() < m; round++) {
+            const unsigned int lim = round == 0 ? std::min(frameStart_, protectFrom) : protectFrom;
+            for (int scanned = 0; scanned < nSlots_ && order.size() < m; scanned++) {
+                const int slot = clock_;
+                clock_ = clock_ + 1 == nSlots_ ? 0 : clock_ + 1;
+                if (slotBrick_[slot] != kEmpty && stampHost_[slot] < lim && mark_[slot] != epoch_) {
+                    mark_[slot] = epoch_;
+                    order.push_back(slot);
+                }
+            }
+        }
     }
-    std::vector<int> order(nSlots_);
-    std::iota(order.begin(), order.end(), 0);
-    if (m > 0)
-        std::nth_element(order.begin(), order.begin() + (m - 1), order.end(), [&](int a, int b) {
-            bool fa = slotBrick_[a] == 0, fb = slotBrick_[b] == 0;
-            if (fa != fb) return fa;
-            return stampHost_[a] < stampHost_[b];
-        });
     size_t need = n * 2 + 2;
     if (need > updCap_) {
         if (h_upd_) cudaFreeHost(h_upd_);
@@ -178,10 +193,9 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
         CKC(cudaMalloc(&d_pairs_, pairsCap_ * sizeof(int2)));
     }
     size_t nu = 0, np = 0;
-    for (size_t k = 0; k < m && np < m; k++) {
+    for (size_t k = 0; k < order.size(); k++) {
         int slot = order[k];
-        if (slotBrick_[slot] != 0) {
-            if (stampHost_[slot] >= protectFrom) continue;   /* in use this frame */
+        if (slotBrick_[slot] != kEmpty) {
             uint64_t old = slotBrick_[slot];
             pageMirror_[old - pageBase_] = -1;
             h_upd_[nu++] = make_int2((int)(old - pageBase_), -1);
@@ -227,19 +241,51 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
     CKC(cudaMemcpyAsync(h_req_, d_req, (size_t)nReq * 8, cudaMemcpyDeviceToHost, s));
     CKC(cudaStreamSynchronize(s));
     requested_ += nReq;
-    size_t cap = std::min<size_t>({(size_t)nReq, (size_t)nSlots_, (size_t)nHost_});
-    std::vector<uint64_t> bricks(h_req_, h_req_ + cap);
-    std::vector<int> hs;
+    std::vector<uint64_t> demand, spec;
+    demand.reserve(nReq);
+    for (unsigned int i = 0; i < nReq; i++) {
+        const uint64_t r = h_req_[i];
+        if (r & VT_REQ_SPECULATIVE) spec.push_back(r & ~VT_REQ_SPECULATIVE);
+        else demand.push_back(r);
+    }
+    speculative_ += (int64_t)spec.size();
     int64_t disk = 0, loaded = 0;
-    vt_status st = ensure_host(bricks, hs, &disk);
-    if (st != VT_OK) return st;
-    /* bricks over the admission cap are re-requested next pass */
-    std::vector<uint64_t> all(h_req_, h_req_ + nReq);
-    std::vector<int> hsAll(hs);
-    hsAll.resize(nReq, -1);
-    /* assign_device handles the first `cap` and resets the rest */
-    st = assign_device(all, hsAll, s, 0xFFFFFFFFu, h2dBytes, &loaded);
-    return st;
+    vt_status st;
+    /* demand requests first: no kernel runs, so any slot may be reused;
+     * bricks over the admission cap are re-requested next pass
+     * (assign_device loads the first `cap` and resets the rest) */
+    if (!demand.empty()) {
+        const size_t cap = std::min<size_t>({demand.size(), (size_t)nSlots_, (size_t)nHost_});
+        std::vector<uint64_t> head(demand.begin(), demand.begin() + cap);
+        std::vector<int> hs;
+        if ((st = ensure_host(head, hs, &disk)) != VT_OK) return st;
+        hs.resize(demand.size(), -1);
+        if ((st = assign_device(demand, hs, s, 0xFFFFFFFFu, h2dBytes, &loaded)) != VT_OK) return st;
+    }
+    /* speculative requests (lookahead): only into free slots or slots this
+     * frame has not used, so they never evict what its rays still need;
+     * the rest go back to absent */
+    if (!spec.empty()) {
+        std::vector<uint64_t> want;
+        want.reserve(spec.size());
+        for (uint64_t p : spec)
+            if (pageMirror_[p - pageBase_] < 0) want.push_back(p);   /* not loaded as a demand request */
+        if (!want.empty()) {
+            /* admit only as many as there are slots they may take, so no
+             * host-tier read is spent on a brick that finds no slot */
+            CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
+            CKC(cudaStreamSynchronize(s));
+            size_t avail = 0;
+            for (int i = 0; i < nSlots_; i++) avail += slotBrick_[i] == kEmpty || stampHost_[i] < frameStart_;
+            const size_t cap = std::min<size_t>({want.size(), avail, (size_t)nHost_});
+            std::vector<uint64_t> head(want.begin(), want.begin() + cap);
+            std::vector<int> hs;
+            if ((st = ensure_host(head, hs, &disk)) != VT_OK) return st;
+            hs.resize(want.size(), -1);
+            if ((st = assign_device(want, hs, s, frameStart_, h2dBytes, &loaded)) != VT_OK) return st;
+        }
+    }
+    return VT_OK;
 }
 
 vt_status BrickCache::prefetch_stage(const std::vector<uint64_t>& bricks, std::vector<uint64_t>& staged,
@@ -307,7 +353,7 @@ void BrickCache::fold_stats(vt_stats& st) {
     st.host_hits = hostHits_; st.host_misses = hostMisses_;
     st.bricks_requested = requested_; st.bricks_loaded_disk = hostMisses_;
     st.bricks_loaded_host = hostHits_; st.bricks_prefetched = prefetched_;
-    st.bricks_hinted = hinted_; st.bricks_staged = staged_;
+    st.bricks_hinted = hinted_; st.bricks_staged = staged_; st.bricks_speculative = speculative_;
     st.launches += launches_ - launchesFolded_;
     launchesFolded_ = launches_;
 }
@@ -315,16 +361,22 @@ vt_status BrickCache::drop() {
     CKC(cudaDeviceSynchronize());
     CKC(cudaMemset(d_page_, 0xFF, pageN_ * 4));
     CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
-    std::fill(slotBrick_.begin(), slotBrick_.end(), 0);
+    std::fill(slotBrick_.begin(), slotBrick_.end(), kEmpty);
+    freeSlots_.resize(nSlots_);
+    for (int i = 0; i < nSlots_; i++) freeSlots_[i] = nSlots_ - 1 - i;
+    clock_ = 0;
     std::fill(stampHost_.begin(), stampHost_.end(), 0);
     std::fill(pageMirror_.begin(), pageMirror_.end(), -1);
     std::fill(hostIndex_.begin(), hostIndex_.end(), -1);
-    std::fill(hostBrick_.begin(), hostBrick_.end(), 0);
+    std::fill(hostBrick_.begin(), hostBrick_.end(), kEmpty);
+    freeHost_.resize(nHost_);
+    for (int i = 0; i < nHost_; i++) freeHost_[i] = nHost_ - 1 - i;
+    hostClock_ = 0;
     std::fill(hostTick_.begin(), hostTick_.end(), 0);
     allResident_ = false;
     return VT_OK;
 }
 
-void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = 0; }
+void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = speculative_ = 0; }
 
 }  // namespace vtrt

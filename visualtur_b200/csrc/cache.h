@@ -73,13 +73,20 @@ private:
     void* d_slab_ = nullptr;
     unsigned int* d_stamp_ = nullptr;
     int nSlots_ = 0;
-    std::vector<uint64_t> slotBrick_;        /* device slot -> brick (0 free) */
+    static constexpr uint64_t kEmpty = ~0ull;  /* slot holds no brick (page 0 is a brick) */
+    std::vector<uint64_t> slotBrick_;        /* device slot -> brick page (kEmpty: free) */
+    std::vector<int> freeSlots_;             /* device slots never filled since init / drop */
+    int clock_ = 0;                          /* victim sweep position over device slots */
+    std::vector<unsigned int> mark_;         /* slot picked in the current call (== epoch_) */
+    unsigned int epoch_ = 0;
     std::vector<int> pageMirror_;            /* host copy of page (>= 0 or -1) */
     std::vector<unsigned int> stampHost_;
     /* host tier */
     unsigned char* h_tier_ = nullptr; void* d_tier_ = nullptr; int nHost_ = 0;
     std::vector<int> hostIndex_;             /* brick -> host slot or -1 */
-    std::vector<uint64_t> hostBrick_;        /* host slot -> brick (0 free) */
+    std::vector<uint64_t> hostBrick_;        /* host slot -> brick page (kEmpty: free) */
+    std::vector<int> freeHost_;              /* host slots never filled since init / drop */
+    int hostClock_ = 0;                      /* victim sweep position over host slots */
     std::vector<uint64_t> hostTick_;
     uint64_t tick_ = 0;
     /* transfer lists */
@@ -89,7 +96,8 @@ private:
     unsigned int pass_ = 0, frameStart_ = 1;
     bool allResident_ = false;
     /* stats */
-    int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0, hinted_ = 0, staged_ = 0;
+    int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0, hinted_ = 0, staged_ = 0,
+            speculative_ = 0;
     int64_t launches_ = 0, launchesFolded_ = 0;
 };
 

@@ -209,12 +209,17 @@ struct Ray {
 
 enum { RAY_RUNNING = 0, RAY_DONE = 1, RAY_SUSPENDED = 2 };
 
-/* requests page `pidx` once per pass (page -1 -> -2) */
-__device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned int pidx) {
-    int old = atomicCAS(&A.br.page[pidx], -1, -2);
+/* Requests page `pidx` once per pass.  A demand request (a ray waits on
+ * the brick) moves the page from absent (-1) or speculatively requested
+ * (-3) to -2; a speculative one (lookahead) from -1 to -3 and is tagged in
+ * the list, so the host loads it only into a slot this frame has not used. */
+__device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned int pidx, bool spec = false) {
+    int old = atomicCAS(&A.br.page[pidx], -1, spec ? VT_PAGE_SPECULATIVE : VT_PAGE_REQUESTED);
+    if (old == VT_PAGE_SPECULATIVE && !spec)
+        old = atomicCAS(&A.br.page[pidx], VT_PAGE_SPECULATIVE, VT_PAGE_REQUESTED) == VT_PAGE_SPECULATIVE ? -1 : old;
     if (old == -1) {
         unsigned int q = atomicAdd(A.ctl.n_req, 1u);
-        if (q < A.ctl.req_cap) A.ctl.req[q] = pidx;
+        if (q < A.ctl.req_cap) A.ctl.req[q] = pidx | (spec ? VT_REQ_SPECULATIVE : 0ull);
         else atomicOr(A.ctl.err, VT_KERR_REQUEST_FULL);
     }
 }
@@ -390,7 +395,7 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
         Samp s; int slot;
         setup_sampler<VTYPE, SLAB>(A, bx, by, bz, pidx, s, &slot);
         if (SLAB && slot < 0) {
-            if (slot == -1) request_brick(A, pidx);
+            if (slot == -1 || slot == VT_PAGE_SPECULATIVE) request_brick(A, pidx);
             cnt[VT_C_DEVMISSES]++;
             return RAY_SUSPENDED;
         }
@@ -440,7 +445,7 @@ __device__ void lookahead_requests(const TraceArgs& A, Ray R, Stk& st, unsigned 
         if (e_level(ent) == Lo) {
             const unsigned int pidx = ((e_x(ent) >> (Lo - Lc)) << (2 * Lc)) | ((e_y(ent) >> (Lo - Lc)) << Lc) |
                                       (e_z(ent) >> (Lo - Lc));
-            if (pidx != last && A.br.page[pidx] == -1) { request_brick(A, pidx); want--; }
+            if (pidx != last && A.br.page[pidx] == -1) { request_brick(A, pidx, true); want--; }
             last = pidx;
             continue;
         }

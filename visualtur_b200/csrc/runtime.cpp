@@ -387,7 +387,9 @@ static vt_status init_handle(vt_handle* h) {
         if (h->opt.preload && (size_t)p.maxElementsCache >= h->leafBricks.size()) {
             if ((s = h->cache->preload(to_pages(h->leafBricks, h->Lc))) != VT_OK) return s;
         }
-        h->req_cap = (unsigned int)std::max<size_t>(h->leafBricks.size(), 1);
+        /* a page enters the list at most twice per pass: speculatively, then
+         * upgraded to a demand request */
+        h->req_cap = (unsigned int)std::max<size_t>(2 * h->leafBricks.size(), 1);
         CK(cudaMalloc(&h->d_req, (size_t)h->req_cap * 8));
     }
     if ((s = alloc_ray_buffers(h)) != VT_OK) return s;
@@ -646,6 +648,7 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
             unsigned int nOut = h->h_ctl->n_out, nReq = h->h_ctl->n_req;
             if (nOut == 0) break;
             if (nOut > h->susp_cap) return fail(VT_ERR_STATE, "suspended-ray list overflow");
+            if (nReq > h->req_cap) return fail(VT_ERR_STATE, "brick request list overflow");
             if (passes >= h->opt.max_passes) return fail(VT_ERR_TIMEOUT, "frame did not finish in %d passes", passes);
             auto ts = std::chrono::steady_clock::now();
             if ((st = h->cache->service(h->d_req, nReq, s, &h2d)) != VT_OK) return st;

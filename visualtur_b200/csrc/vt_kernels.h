@@ -14,6 +14,10 @@
 #define VT_KERR_NOTRESIDENT 2u  /* resident mode met a brick with no slot */
 #define VT_KERR_SUSPEND_FULL 4u /* suspended-ray list overflowed */
 #define VT_KERR_REQUEST_FULL 8u /* brick request list overflowed */
+/* page-table states besides a slot index: -1 absent, and */
+#define VT_PAGE_REQUESTED (-2)     /* a ray waits on the brick */
+#define VT_PAGE_SPECULATIVE (-3)   /* requested ahead of need (lookahead) */
+#define VT_REQ_SPECULATIVE (1ull << 63)   /* request-list tag of a speculative request */
 
 /* counter slots in DevCtl::counters */
 enum {
