@@ -559,7 +559,7 @@ PAGING_CANDIDATES = ((8, 2), (4, 2), (2, 2), (1, 2), (1, 0))   # (frames per lau
 HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
 
 
-def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=48):
+def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
     """Frames per launch, lookahead and the prefetch-hint threshold for an
     out-of-core fly-through: each candidate renders the same `frames`
     frames (another stretch of the path than the timed one) from a cold
