@@ -40,8 +40,11 @@ template <class OutT>
 static void read_box(const vt_volume* v, const int s[3], const int e[3], OutT* out) {
     int64_t dim[3];
     for (int a = 0; a < 3; a++) dim[a] = std::llabs((long long)e[a] - s[a]);
-    memset(out, 0, (size_t)(dim[0] * dim[1] * dim[2]) * sizeof(OutT));
     const int64_t* D = v->dims;
+    /* a box inside the volume is overwritten completely: no zeroing */
+    bool inside = true;
+    for (int a = 0; a < 3; a++) inside = inside && s[a] >= 0 && e[a] >= s[a] && e[a] <= D[a];
+    if (!inside) memset(out, 0, (size_t)(dim[0] * dim[1] * dim[2]) * sizeof(OutT));
     if (s[0] >= D[0] || s[1] >= D[1] || s[2] >= D[2] || e[0] < 0 || e[1] < 0 || e[2] < 0) return;
     int64_t oo[3], off[3], dr[3];
     for (int a = 0; a < 3; a++) {
@@ -50,8 +53,22 @@ static void read_box(const vt_volume* v, const int s[3], const int e[3], OutT* o
         dr[a] = e[a] > D[a] ? D[a] - off[a] : e[a] - off[a];
         if (dr[a] <= 0) return;
     }
+    /* rows are short and far apart (one per y, x): fetch PF rows ahead,
+     * walking a second (x, y) cursor */
+    const int PF = 8;
+    const size_t es = v->esize(), rowBytes = (size_t)dr[2] * es;
+    int64_t pa = 0, pb = 0;
+    auto prefetch_next = [&]() {
+        if (pa >= dr[0]) return;
+        const unsigned char* q = v->data + (size_t)(((off[0] + pa) * D[1] + (off[1] + pb)) * D[2] + off[2]) * es;
+        for (size_t c = 0; c < rowBytes; c += 64) __builtin_prefetch(q + c);
+        __builtin_prefetch(q + rowBytes - 1);
+        if (++pb == dr[1]) { pb = 0; pa++; }
+    };
+    for (int i = 0; i < PF; i++) prefetch_next();
     for (int64_t a = 0; a < dr[0]; a++)
         for (int64_t b = 0; b < dr[1]; b++) {
+            prefetch_next();
             size_t src = (size_t)(((off[0] + a) * D[1] + (off[1] + b)) * D[2] + off[2]);
             OutT* dst = out + ((oo[0] + a) * dim[1] + (oo[1] + b)) * dim[2] + oo[2];
             if (v->vtype == VT_F32) {
