@@ -50,10 +50,14 @@ __global__ void k_page_update(int* page, const int2* upd, int n, unsigned int* s
 BrickCache::~BrickCache() {
     cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_);
     if (h_tier_) cudaFreeHost(h_tier_);
-    if (h_pairs_) cudaFreeHost(h_pairs_);
-    if (h_upd_) cudaFreeHost(h_upd_);
+    for (Xfer& X : xf_) {
+        if (X.ev) cudaEventSynchronize(X.ev), cudaEventDestroy(X.ev);
+        if (X.hp) cudaFreeHost(X.hp);
+        if (X.hu) cudaFreeHost(X.hu);
+        cudaFree(X.dp); cudaFree(X.du);
+    }
     if (h_req_) cudaFreeHost(h_req_);
-    cudaFree(d_pairs_); cudaFree(d_upd_);
+
 }
 
 vt_status BrickCache::init(const CacheConfig& c) {
@@ -103,10 +107,11 @@ void BrickCache::read_brick(uint64_t page, void* dst) const {
     volume_read_native(cfg_.vol, s, e, dst);
 }
 
-vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads) {
+vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads,
+                                  uint64_t protectTick) {
     const size_t n = bricks.size();
     hslot.assign(n, -1);
-    const uint64_t callStart = tick_ + 1;
+    const uint64_t callStart = protectTick ? protectTick : tick_ + 1;
     std::vector<size_t> miss;
     for (size_t i = 0; i < n; i++) {
         int hs = hostIndex_[bricks[i] - pageBase_];
@@ -148,9 +153,12 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
 }
 
 vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
-                                    unsigned int protectFrom, double* h2d, int64_t* loaded) {
+                                    unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync) {
     const size_t n = bricks.size();
     if (n == 0) return VT_OK;
+    Xfer& X = xf_[xfNext_];
+    xfNext_ ^= 1;
+    if (X.pending) { CKC(cudaEventSynchronize(X.ev)); X.pending = false; }
     /* bricks with a host-tier copy, at most one per device slot */
     size_t m = 0;
     while (m < n && m < (size_t)nSlots_ && hslot[m] >= 0) m++;
@@ -178,20 +186,22 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
         }
     }
     size_t need = n * 2 + 2;
-    if (need > updCap_) {
-        if (h_upd_) cudaFreeHost(h_upd_);
-        cudaFree(d_upd_);
-        updCap_ = need * 2;
-        CKC(cudaHostAlloc((void**)&h_upd_, updCap_ * sizeof(int2), cudaHostAllocDefault));
-        CKC(cudaMalloc(&d_upd_, updCap_ * sizeof(int2)));
+    if (need > X.ucap) {
+        if (X.hu) cudaFreeHost(X.hu);
+        cudaFree(X.du);
+        X.ucap = need * 2;
+        CKC(cudaHostAlloc((void**)&X.hu, X.ucap * sizeof(int2), cudaHostAllocDefault));
+        CKC(cudaMalloc(&X.du, X.ucap * sizeof(int2)));
     }
-    if (n > pairsCap_) {
-        if (h_pairs_) cudaFreeHost(h_pairs_);
-        cudaFree(d_pairs_);
-        pairsCap_ = n * 2;
-        CKC(cudaHostAlloc((void**)&h_pairs_, pairsCap_ * sizeof(int2), cudaHostAllocDefault));
-        CKC(cudaMalloc(&d_pairs_, pairsCap_ * sizeof(int2)));
+    if (n > X.pcap) {
+        if (X.hp) cudaFreeHost(X.hp);
+        cudaFree(X.dp);
+        X.pcap = n * 2;
+        CKC(cudaHostAlloc((void**)&X.hp, X.pcap * sizeof(int2), cudaHostAllocDefault));
+        CKC(cudaMalloc(&X.dp, X.pcap * sizeof(int2)));
     }
+    int2* const h_upd_ = X.hu;
+    int2* const h_pairs_ = X.hp;
     size_t nu = 0, np = 0;
     for (size_t k = 0; k < order.size(); k++) {
         int slot = order[k];
@@ -213,19 +223,25 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
         if (pageMirror_[bricks[k] - pageBase_] < 0) h_upd_[nu++] = make_int2((int)(bricks[k] - pageBase_), -1);
     if (np) {
         launches_++;
-        CKC(cudaMemcpyAsync(d_pairs_, h_pairs_, np * sizeof(int2), cudaMemcpyHostToDevice, s));
-        k_fill_bricks<<<(unsigned int)np, 256, 0, s>>>((const unsigned char*)d_tier_, slotBytes_, d_pairs_,
+        CKC(cudaMemcpyAsync(X.dp, h_pairs_, np * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_fill_bricks<<<(unsigned int)np, 256, 0, s>>>((const unsigned char*)d_tier_, slotBytes_, X.dp,
                                                        (unsigned char*)d_slab_);
         CKC(cudaGetLastError());
     }
     if (nu) {
         launches_++;
-        CKC(cudaMemcpyAsync(d_upd_, h_upd_, nu * sizeof(int2), cudaMemcpyHostToDevice, s));
-        k_page_update<<<(unsigned int)((nu + 255) / 256), 256, 0, s>>>(d_page_, d_upd_, (int)nu, d_stamp_, pass_ + 1);
+        CKC(cudaMemcpyAsync(X.du, h_upd_, nu * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_page_update<<<(unsigned int)((nu + 255) / 256), 256, 0, s>>>(d_page_, X.du, (int)nu, d_stamp_, pass_ + 1);
         CKC(cudaGetLastError());
     }
-    /* the pinned lists are reused by the next call */
-    CKC(cudaStreamSynchronize(s));
+    /* the pinned lists are reused by the call after next */
+    if (!X.ev) CKC(cudaEventCreateWithFlags(&X.ev, cudaEventDisableTiming));
+    CKC(cudaEventRecord(X.ev, s));
+    X.pending = true;
+    if (sync) {
+        CKC(cudaStreamSynchronize(s));
+        xf_[0].pending = xf_[1].pending = false;
+    }
     *h2d += (double)np * (double)slotBytes_;
     *loaded += (int64_t)np;
     return VT_OK;
@@ -255,12 +271,21 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
      * bricks over the admission cap are re-requested next pass
      * (assign_device loads the first `cap` and resets the rest) */
     if (!demand.empty()) {
+        /* in chunks: the host-tier reads of one chunk overlap the device fill
+         * of the one before; host slots filled in this service stay put */
+        const size_t kChunk = 8192;
         const size_t cap = std::min<size_t>({demand.size(), (size_t)nSlots_, (size_t)nHost_});
-        std::vector<uint64_t> head(demand.begin(), demand.begin() + cap);
-        std::vector<int> hs;
-        if ((st = ensure_host(head, hs, &disk)) != VT_OK) return st;
-        hs.resize(demand.size(), -1);
-        if ((st = assign_device(demand, hs, s, 0xFFFFFFFFu, h2dBytes, &loaded)) != VT_OK) return st;
+        const uint64_t svcStart = tick_ + 1;
+        for (size_t c0 = 0; c0 < cap; c0 += kChunk) {
+            const size_t c1 = std::min(cap, c0 + kChunk);
+            const bool last = c1 == cap;
+            std::vector<uint64_t> head(demand.begin() + c0, demand.begin() + c1);
+            std::vector<int> hs;
+            if ((st = ensure_host(head, hs, &disk, svcStart)) != VT_OK) return st;
+            if (last) head.insert(head.end(), demand.begin() + cap, demand.end());   /* reset to absent */
+            hs.resize(head.size(), -1);
+            if ((st = assign_device(head, hs, s, 0xFFFFFFFFu, h2dBytes, &loaded, last)) != VT_OK) return st;
+        }
     }
     /* speculative requests (lookahead): only into free slots or slots this
      * frame has not used, so they never evict what its rays still need;

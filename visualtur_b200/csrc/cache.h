@@ -60,9 +60,14 @@ public:
     size_t slot_bytes() const { return slotBytes_; }
 
 private:
-    vt_status ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads);
+    /* protectTick: host slots touched at or after this tick are not evicted
+     * (0: those touched in this call) */
+    vt_status ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads,
+                          uint64_t protectTick = 0);
+    /* sync = false leaves the fill running; the transfer lists are double
+     * buffered, so the next call overlaps it */
     vt_status assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
-                            unsigned int protectFrom, double* h2d, int64_t* loaded);
+                            unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync = true);
     void read_brick(uint64_t code, void* dst) const;
 
     CacheConfig cfg_;
@@ -90,8 +95,12 @@ private:
     std::vector<uint64_t> hostTick_;
     uint64_t tick_ = 0;
     /* transfer lists */
-    int2* h_pairs_ = nullptr; int2* d_pairs_ = nullptr; size_t pairsCap_ = 0;
-    int2* h_upd_ = nullptr; int2* d_upd_ = nullptr; size_t updCap_ = 0;
+    struct Xfer {
+        int2* hp = nullptr; int2* dp = nullptr; size_t pcap = 0;   /* (host slot, device slot) pairs */
+        int2* hu = nullptr; int2* du = nullptr; size_t ucap = 0;   /* (page, slot) updates */
+        cudaEvent_t ev = nullptr; bool pending = false;            /* last use still on the GPU */
+    } xf_[2];
+    int xfNext_ = 0;
     unsigned long long* h_req_ = nullptr; size_t reqCap_ = 0;
     unsigned int pass_ = 0, frameStart_ = 1;
     bool allResident_ = false;
