@@ -567,6 +567,28 @@ def frame_deltas(per_frame):
     return out
 
 
+# ----------------------------------------------------------------------------- replicas
+def replica_first_frame(rank, warmup, steps):
+    """Replicas render disjoint stretches of the workload: rank r starts at
+    frame r * (warmup + steps) (no data is exchanged between GPUs)."""
+    return rank * (warmup + steps)
+
+
+def max_over_ranks(dist, torch, value, device):
+    """The largest of the ranks' values (a time in ms): a job is as slow as
+    its slowest replica.  Every rank must call it at the same point."""
+    if not dist:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(rays_per_rank, world, t_max_ms):
+    """Whole-job throughput: every rank's rays over the slowest rank's time."""
+    return rays_per_rank * world / (t_max_ms * 1e-3)
+
+
 def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=False, plain=False):
     if "views" in cfg:
         return ViewLauncher(wl, r, cfg, torch, dev, stream, predictor=predictor, warm=warm, plain=plain)
@@ -656,7 +678,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     M = MODES[args.mode]
     wl = Workload(cfg, torch, dev, work, mode=args.mode, warm=args.warm)
     stream = torch.cuda.Stream(device=dev)
-    frame0 = rank * (args.warmup + args.steps)   # replicas render distinct frames
+    frame0 = replica_first_frame(rank, args.warmup, args.steps)
     batch = 1 if (cfg["resident"] or "views" in cfg) else M["batch"]
     P = wl.train_prefetcher(torch) if (M["learned"] and not cfg["resident"] and not args.no_learned) else None
     tune = None
@@ -687,12 +709,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
     ld = frame_deltas(per)
     trace_tot = sum(s["ms_trace_last_frame"] for s in per)
     rays_rank = sum(L.rays(cams) for _, _, cams, _ in launches)
-    t_max = tot_ms
-    if dist:
-        t = torch.tensor([tot_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = rays_rank * world / (t_max * 1e-3)
+    t_max = max_over_ranks(dist, torch, tot_ms, dev)
+    value = replica_value(rays_rank, world, t_max)
     # end to end through the public API: poses in, RGB8 images back in pinned host memory
     e2e_steps = max(batch, 2 * batch if batch > 1 else (4 if "views" in cfg else 30))
     maxb = max(b.numel() for b, _ in L.outputs(L.cams(frame0, batch)))
@@ -710,7 +728,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
                 d2h += nb
             e2e_rays += L.rays(cams)
             stream.synchronize()
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(dist, torch, (time.perf_counter() - t0) * 1e3, dev) * 1e-3
     import ctypes
     per_view = ctypes.sizeof(wl.vt.vt_camera)
     views_per_step = cfg["views"]["n"] if "views" in cfg else 1
@@ -727,8 +745,9 @@ def run_ours(args, cfg, rank, world, torch, dist):
         Lp = make_launcher(wl, rp, cfg, torch, dev, stream, 1, plain=True)
         pms, pper, _, _ = timed_frames(Lp, frame0, args.warmup, args.steps, dist, label="plain")
         ps = rp.stats()
-        plain = {"value": round(rays_rank * world / (sum(pms) * 1e-3), 1), "unit": "rays/s",
-                 "ms_per_step": round(sum(pms) / args.steps, 4),
+        p_max = max_over_ranks(dist, torch, sum(pms), dev)
+        plain = {"value": round(replica_value(rays_rank, world, p_max), 1), "unit": "rays/s",
+                 "ms_per_step": round(p_max / args.steps, 4),
                  "stall_ms_per_step": round(sum(s["ms_stall_last_frame"] for s in pper) / args.steps, 4),
                  "passes_per_step": round(sum(s["passes"] for s in pper) / args.steps, 3),
                  "device_hit_rate": round(ps["device_hits"] / max(1, ps["device_hits"] + ps["device_misses"]), 5),
