@@ -358,11 +358,12 @@ def sample_camera(cfg, step):
     return step_views(cfg, step)[0] if "views" in cfg else frame_camera(vt, cfg, step)
 
 
-def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0):
+def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0, octree=None, per_ray=None):
     """Oracle (CPU restatement of the reference algorithm) on a bounded ray
-    sample of step `step`'s camera; returns rays/s."""
+    sample of step `step`'s camera; returns rays/s (with "per_ray_s", the
+    probe's seconds per ray, to size later samples without probing)."""
     from oracle import oracle as orc
-    o = orc.Octree(octree_path)
+    o = octree if octree is not None else orc.Octree(octree_path)
     c = sample_camera(cfg, step)
     cam = orc.Camera(c.H, c.W, cfg["dist"], cfg["fov"], cfg["fov"])
     for f in ("look", "up", "right", "position"):
@@ -371,10 +372,11 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0):
     n = c.W * c.H
     stride = 1
     # probe a sparse sample, then size the sample to the time budget
-    t0 = time.perf_counter()
-    orc.render(o, wl.volume, cam, cfg["levelO"], cfg["levelC"], cfg["inc"], nthreads=nthreads, ray_stride=257)
-    dt = max(time.perf_counter() - t0, 1e-6)
-    per_ray = dt / (n // 257 + 1)
+    if per_ray is None:
+        t0 = time.perf_counter()
+        orc.render(o, wl.volume, cam, cfg["levelO"], cfg["levelC"], cfg["inc"], nthreads=nthreads, ray_stride=257)
+        dt = max(time.perf_counter() - t0, 1e-6)
+        per_ray = dt / (n // 257 + 1)
     stride = max(1, int(math.ceil(n * per_ray / budget_s)))
     t0 = time.perf_counter()
     reps = 0
@@ -389,7 +391,7 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0):
     threads = nthreads or os.cpu_count()
     return {"value": round(rays / el, 1), "unit": "rays/s", "cores": threads, "kind": "port",
             "sample": "%d x every %d-th ray of a %dx%d view of step %d (%d rays, %.1f s)" %
-                      (reps, stride, c.W, c.H, step, rays, el)}
+                      (reps, stride, c.W, c.H, step, rays, el), "per_ray_s": el / max(rays, 1)}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -804,7 +806,9 @@ def run_ours(args, cfg, rank, world, torch, dist):
         if tune["bricks"]:
             line["autotune"]["bricks"] = tune["bricks"]
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, step=frame0 + args.warmup)
+        cb = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, step=frame0 + args.warmup)
+        cb.pop("per_ray_s")
+        line["cpu_baseline"] = cb
     return line
 
 
@@ -818,9 +822,14 @@ def run_reference(args, cfg, rank, world, torch):
         n = sum(c.W * c.H for c in step_views(cfg, args.warmup))
     else:
         n = cfg["W"] * cfg["H"]
-    vals = []
+    # the whole run samples about --ref-total seconds of CPU rendering
+    from oracle import oracle as orc
+    octree = orc.Octree(wl.octree_path)
+    budget = max(0.1, min(args.ref_budget, args.ref_total / (args.warmup + args.steps)))
+    vals, per_ray = [], None
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(cfg, wl, wl.octree_path, args.ref_budget, step=i)
+        cb = cpu_baseline(cfg, wl, wl.octree_path, budget, step=i, octree=octree, per_ray=per_ray)
+        per_ray = cb.pop("per_ray_s")
         if i >= args.warmup:
             vals.append(cb)
     rays_s = statistics.median(v["value"] for v in vals)
@@ -850,7 +859,8 @@ def main():
     ap.add_argument("--config", default=os.environ.get("VT_BENCH_CONFIG", "c2"), choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0)
-    ap.add_argument("--ref-budget", type=float, default=6.0)
+    ap.add_argument("--ref-budget", type=float, default=6.0, help="reference arm: CPU seconds per step at most")
+    ap.add_argument("--ref-total", type=float, default=150.0, help="reference arm: CPU seconds over all steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="best", choices=sorted(MODES))
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-LRU comparison run")
@@ -867,7 +877,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
-    if world > 1:
+    if world > 1 and args.impl == "reference":
+        if rank != 0:
+            return                  # the reference arm runs on rank 0's host cores only
+    elif world > 1:
         import datetime
         import torch.distributed as tdist
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
