@@ -103,7 +103,7 @@ CONFIGS = {
 # prefetch hints for the next batch, kernel knobs from the autotuner
 MODES = {
     "plain": dict(opts=dict(persistent=0, lookahead=0, use_graph=0), batch=1, learned=False, autotune=False),
-    "best": dict(opts=dict(persistent=1, lookahead=2, use_graph=1, pops=8, blocks_per_sm=8), batch=8,
+    "best": dict(opts=dict(persistent=1, lookahead=2, use_graph=1, pops=32, blocks_per_sm=8), batch=8,
                  learned=True, autotune=True),
 }
 

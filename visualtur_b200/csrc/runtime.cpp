@@ -328,7 +328,7 @@ extern "C" void vt_default_options(vt_options* o) {
     o->record_hits = 1;
     o->persistent = 0;
     o->blocks_per_sm = 8;
-    o->pops = 8;
+    o->pops = 32;
     o->preload = 1;
     o->use_graph = 1;
     o->refine = 0;
