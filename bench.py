@@ -2,7 +2,7 @@
 """Benchmark: rays/s and ms/frame of the isosurface ray caster on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config c2|c1|c3|c2s|c3s]
-                  [--mode best|plain] [--impl ours|reference]
+                  [--mode best|plain] [--impl ours|reference]   (also c4, c5, c5s)
 
 A step is one rendered frame of the workload (one batch of views for c3):
   c2 (default): the 2048^3 float32 out-of-core fly-through -- 256 seeded
@@ -16,7 +16,10 @@ A step is one rendered frame of the workload (one batch of views for c3):
       sphere of radius 2500-3500 looking into the inner half, resolutions
       drawn from {256^2, 512^2, 1024^2, 1920x1080, 2048^2}; the autotuner
       also picks the brick edge {8, 16, 32}.
-  c2s / c3s: c2 / c3 on a 1024^3 volume (profiling and quick checks).
+  c4: the c2 volume on a held-out 300-frame spline (the learned-prefetch
+      judgement: hit rate, stall per frame, same pixels as plain).
+  c5: 4096^3 uint8 fractal, 32^3 bricks, 16 GB cache, 600-frame spline.
+  c2s / c3s / c5s: c2 / c3 / c5 at half the edge (profiling and quick checks).
 value = rays of all ranks / device time (CUDA events, max over ranks).
 Multi-GPU: replicas only -- each rank renders its own frames, no
 collective on the data path ("scaling": "weak").
@@ -60,6 +63,14 @@ CONFIGS = {
                dist=50.0, resident=0, l2flush=False, orbit=(3000.0, 1.2), dev_bytes=4 << 30,
                host_bytes=16 << 30, blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05)),
     # 64 seeded views per launch, mixed resolutions, on the c2 volume
+    # the learned-prefetch judgement: the c2 volume on a held-out spline
+    "c4": dict(workload="2048^3 f32 blobs+noise (the c2 volume), held-out 300-frame Catmull-Rom spline through 12 "
+                        "seeded control points at r 2500-3500 looking into the inner half, 1920x1080, 4 GB device "
+                        "cache, 16 GB pinned host tier, prefetch network trained on 20 000 poses of other "
+                        "fly-throughs, timed from a cold cache",
+               gen="blobs", seed=2048, n=2048, iso=0.6, levelC=7, levelO=9, inc=3, W=1920, H=1080, fov=30.0,
+               dist=50.0, resident=0, l2flush=False, orbit=None, dev_bytes=4 << 30, host_bytes=16 << 30,
+               blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05), path=dict(frames=300, ctrl=12, r=(2500.0, 3500.0))),
     "c3": dict(workload="2048^3 f32 blobs+noise (the c2 volume), 64 views per launch at seeded random poses "
                         "on a sphere r in [2500,3500] looking into the inner half, resolutions drawn from "
                         "{256^2, 512^2, 1024^2, 1920x1080, 2048^2}; 4 GB device cache, 16 GB pinned host tier, "
@@ -444,7 +455,7 @@ class Launcher:
             for c, p in zip(win, probs):
                 cache[self._key(c)] = p
         probs = np.max(np.stack([cache[self._key(c)] for c in cams]), axis=0)
-        self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
+        self.r.prefetch_hint(self.P.new_bricks_for(probs, self.thr))
         self.hint_s += time.perf_counter() - t0
 
     def launch(self, cams, next_cams=(), f=None):
@@ -494,7 +505,7 @@ class ViewLauncher:
         from visualtur_b200 import prefetch as pf
         feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for views in items for c in views])
         probs = self.P.predict(self.torch, feats).max(axis=0)
-        self.r.prefetch_hint(self.P.bricks_for(probs, self.thr))
+        self.r.prefetch_hint(self.P.new_bricks_for(probs, self.thr))
         self.hint_s += time.perf_counter() - t0
 
     def launch(self, items, next_items=(), f=None):
@@ -528,6 +539,8 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
         torch.cuda.synchronize()
         if not L.cfg["resident"] and not L.warm:
             r.drop_cache()     # every timed run starts from a cold cache: all loading is timed
+            if L.P is not None:
+                L.P.reset_hints()
         r.reset_stats()
         launches = []
         f = frame0 + warmup
@@ -591,6 +604,14 @@ def replica_value(rays_per_rank, world, t_max_ms):
     return rays_per_rank * world / (t_max_ms * 1e-3)
 
 
+def frame_digest(r, cam):
+    """SHA-256 of the float RGBA frame renderer `r` makes from `cam`."""
+    import hashlib
+    r.set_camera(cam)
+    rgba, _ = r.render_host(rgb8=False)
+    return hashlib.sha256(rgba.tobytes()).hexdigest()
+
+
 def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=False, plain=False):
     if "views" in cfg:
         return ViewLauncher(wl, r, cfg, torch, dev, stream, predictor=predictor, warm=warm, plain=plain)
@@ -614,6 +635,8 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
         L = make_launcher(wl, wl.r, cfg, torch, dev, stream, b, predictor=P)
         L.thr = thr
         wl.r.drop_cache()
+        if P is not None:
+            P.reset_hints()
         a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             torch.cuda.synchronize()
@@ -741,9 +764,18 @@ def run_ours(args, cfg, rank, world, torch, dist):
                    "(vt_render / vt_render_batch) plus the D2H copy of every RGB8 image"}
     # the plain LRU renderer on the same steps, for comparison
     plain = None
+    check = None
     if args.mode != "plain" and not cfg["resident"] and not args.no_plain:
+        # the same frames from both renderers must be identical
+        check = {"frames": [frame0 + args.warmup + k * max(1, args.steps // 4) for k in range(4)]}
+        if "views" not in cfg:
+            check["best"] = [frame_digest(wl.r, frame_camera(wl.vt, cfg, f)) for f in check["frames"]]
         wl.r.close()
         rp = wl.renderer("plain")
+        if "views" not in cfg:
+            check["plain"] = [frame_digest(rp, frame_camera(wl.vt, cfg, f)) for f in check["frames"]]
+            rp.drop_cache()
+            rp.reset_stats()
         Lp = make_launcher(wl, rp, cfg, torch, dev, stream, 1, plain=True)
         pms, pper, _, _ = timed_frames(Lp, frame0, args.warmup, args.steps, dist, label="plain")
         ps = rp.stats()
@@ -797,6 +829,9 @@ def run_ours(args, cfg, rank, world, torch, dist):
     }
     if plain:
         line["plain_lru"] = plain
+        if check and "best" in check:
+            plain["same_pixels"] = check["best"] == check["plain"]
+            plain["pixels_checked_frames"] = check["frames"]
     if P is not None:
         line["learned_prefetch"] = wl.train_info
     if tune:
@@ -888,7 +923,8 @@ def main():
         dist = tdist
     cfg = CONFIGS[args.config]
     if args.steps is None:
-        args.steps = (300 if cfg["orbit"] else 600 if cfg.get("path") else 6 if "views" in cfg else 200)
+        args.steps = (300 if cfg["orbit"] else cfg["path"]["frames"] if cfg.get("path") else
+                      6 if "views" in cfg else 200)
     if args.impl == "reference":
         line = run_reference(args, cfg, rank, world, torch)
     else:

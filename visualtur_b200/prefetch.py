@@ -153,6 +153,24 @@ class Prefetcher:
         """sorted brick codes of every node whose probability exceeds threshold"""
         return self.bricks[np.asarray(probs)[self.brick_node] > threshold]
 
+    def reset_hints(self):
+        """Forget what was hinted (after the renderer's cache was dropped)."""
+        self._last_hint = None
+
+    def new_bricks_for(self, probs, threshold, refresh=32):
+        """bricks_for, less those already hinted in the last `refresh` calls:
+        once a brick has been hinted it is loaded (or was resident), so
+        repeating it only costs the renderer a lookup.  Bricks come back
+        after `refresh` calls, in case the cache has evicted them since."""
+        if getattr(self, "_last_hint", None) is None or len(self._last_hint) != len(self.bricks):
+            self._last_hint = np.full(len(self.bricks), -(1 << 30), np.int64)
+            self._calls = 0
+        self._calls += 1
+        sel = np.asarray(probs)[self.brick_node] > threshold
+        sel &= self._last_hint <= self._calls - refresh
+        self._last_hint[sel] = self._calls
+        return self.bricks[sel]
+
 
 def collect_traces(renderer, n, W, H, fov, rng, paths, frames, r_lo, r_hi, level=TRACE_LEVEL, dist=50.0):
     """(pose features, marched-node targets) pairs from `paths` random
