@@ -246,8 +246,10 @@ vt_status vt_get_trace(vt_handle* h, uint32_t* bits, int64_t nwords);
 vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n, int64_t* loaded, void* stream);
 
 /* Prefetch hint for the frame after the next vt_render: during that call
- * the bricks' host-tier reads run while its kernels render, and their
- * device fill follows its last pass (never evicting bricks it used). */
+ * the bricks' host-tier reads run while its first pass renders (in hint
+ * order, as many as finish before the pass does; the rest are dropped),
+ * and their device fill follows its last pass (never evicting bricks it
+ * used). */
 vt_status vt_prefetch_hint(vt_handle* h, const uint64_t* bricks, int64_t n);
 
 /* Bricks (codes at levelCubes) that hold candidate nodes of the octree,

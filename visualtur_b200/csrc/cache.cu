@@ -314,18 +314,24 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
 }
 
 vt_status BrickCache::prefetch_stage(const std::vector<uint64_t>& bricks, std::vector<uint64_t>& staged,
-                                      std::vector<int>& hslot) {
-    staged.clear();
+                                      std::vector<int>& hslot, bool append, uint64_t protectTick) {
+    if (!append) { staged.clear(); hslot.clear(); }
     const size_t cap = (size_t)std::min(nSlots_, nHost_);
     hinted_ += (int64_t)bricks.size();
+    std::vector<uint64_t> part;
     for (uint64_t b : bricks) {
-        if (staged.size() >= cap) break;
-        if (pageMirror_[b - pageBase_] < 0) staged.push_back(b);
+        if (staged.size() + part.size() >= cap) break;
+        if (pageMirror_[b - pageBase_] < 0) part.push_back(b);
     }
-    staged_ += (int64_t)staged.size();
-    if (staged.empty()) { hslot.clear(); return VT_OK; }
+    staged_ += (int64_t)part.size();
+    if (part.empty()) return VT_OK;
     int64_t disk = 0;
-    return ensure_host(staged, hslot, &disk);
+    std::vector<int> hs;
+    vt_status st = ensure_host(part, hs, &disk, protectTick);
+    if (st != VT_OK) return st;
+    staged.insert(staged.end(), part.begin(), part.end());
+    hslot.insert(hslot.end(), hs.begin(), hs.end());
+    return VT_OK;
 }
 
 vt_status BrickCache::prefetch_commit(const std::vector<uint64_t>& staged, const std::vector<int>& hslot,

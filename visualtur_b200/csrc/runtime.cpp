@@ -637,7 +637,17 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
     std::vector<uint64_t> staged;
     std::vector<int> stagedSlots;
     if (slabMode && !h->hint.empty()) {
-        if ((st = h->cache->prefetch_stage(h->hint, staged, stagedSlots)) != VT_OK) return st;
+        /* stage in small parts only while pass 0 still runs on the GPU: the
+         * host-tier reads then never lengthen the frame; the rest of the
+         * hint is dropped */
+        const size_t kPart = 1024;
+        const uint64_t protect = h->cache->host_tick() + 1;
+        for (size_t p0 = 0; p0 < h->hint.size(); p0 += kPart) {
+            std::vector<uint64_t> part(h->hint.begin() + p0, h->hint.begin() + std::min(h->hint.size(), p0 + kPart));
+            if ((st = h->cache->prefetch_stage(part, staged, stagedSlots, true, protect)) != VT_OK) return st;
+            if (cudaEventQuery(h->ev[1]) != cudaErrorNotReady) break;
+        }
+        if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();   /* the query's answer, not a fault */
         h->hint.clear();
     }
     if (!allResident) {
