@@ -78,3 +78,68 @@ def test_cpp_facade_compiles_and_matches(workdir):
     want.append("%s %s" % (hexf(st["h"]), hexf(st["w"])))
     assert lines[:5] == want
     assert lines[5] == "ok %d" % vt.VT_ERR_UNSUPPORTED
+
+
+RENDER_PROG = r'''
+#define VT_REFERENCE_NAMES
+#include "visualtur.hpp"
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <vector>
+
+/* shaped like src/testVisualTur.cu:28-110: parameters, a camera move, a
+ * device pixel buffer, updateVisibleCubes, copy back, strafe, again */
+int main(int argc, char** argv) {
+    visualTurParams_t p;
+    p.W = 96; p.H = 96; p.fov_H = 30.0f; p.fov_W = 30.0f; p.distance = 50.0f; p.numRayPx = 1;
+    p.maxElementsCache = 512; p.maxElementsCache_CPU = 512;
+    p.dimCubeCache.x = p.dimCubeCache.y = p.dimCubeCache.z = 8; p.cubeInc = 3; p.levelCubes = 3;
+    p.hdf5File = argv[1]; p.dataset_name = (char*)"value"; p.octreeFile = argv[2]; p.octreeLevel = 4;
+    visualTur* v = new visualTur(p);
+    float3 mv; mv.x = 31.5f; mv.y = 31.5f; mv.z = 181.5f;
+    v->camera_Move(mv);
+    float* screenG = nullptr;
+    if (cudaMalloc(&screenG, sizeof(float) * p.W * p.H * 4) != cudaSuccess) return 3;
+    std::vector<float> screenC(p.W * p.H * 4);
+    FILE* f = fopen(argv[3], "wb");
+    for (int m = 0; m < 2; m++) {
+        v->updateVisibleCubes(screenG);
+        if (cudaMemcpy(screenC.data(), screenG, screenC.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return 4;
+        fwrite(screenC.data(), 4, screenC.size(), f);
+        v->camera_StrafeRight(0.5f);
+    }
+    fclose(f);
+    cudaFree(screenG);
+    delete v;
+    printf("rendered\n");
+    return 0;
+}
+'''
+
+
+@pytest.mark.gpu
+def test_cpp_facade_renders_like_the_reference_program(workdir, cuda):
+    src = os.path.join(workdir, "facade_render.cpp")
+    exe = os.path.join(workdir, "facade_render")
+    open(src, "w").write(RENDER_PROG)
+    inc = os.path.join(F.ROOT, "include")
+    libdir = os.path.dirname(vt.LIB_PATH)
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", inc, "-I", "/usr/local/cuda/include", src, "-o", exe,
+                        "-L", libdir, "-lvt", "-Wl,-rpath," + libdir, "-L", "/usr/local/cuda/lib64", "-lcudart"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    c = F.CASES["s64"]
+    vol = F.case_volume("s64")
+    h5 = os.path.join(workdir, "facade_s64.h5")
+    vt.FileManager.CreateFile(vol, h5)
+    octf = F.case_octree("s64", workdir)
+    out = os.path.join(workdir, "facade_frames.f32")
+    run = subprocess.run([exe, h5, octf, out], capture_output=True, text=True)
+    assert run.returncode == 0 and "rendered" in run.stdout, run.stdout + run.stderr
+    got = np.fromfile(out, np.float32).reshape(2, c["W"] * c["H"], 4)
+    cam = F.oracle_camera("s64")
+    o = orc.Octree(octf)
+    for m in range(2):
+        want = orc.render(o, vol, cam, c["levelO"], c["levelC"], c["inc"])["rgba"]
+        assert np.array_equal(got[m].view(np.uint32), want.view(np.uint32))
+        cam.StrafeRight(0.5)
