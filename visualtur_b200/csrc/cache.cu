@@ -107,6 +107,8 @@ void BrickCache::read_brick(uint64_t page, void* dst) const {
     volume_read_native(cfg_.vol, s, e, dst);
 }
 
+int BrickCache::host_threads() const { return cfg_.hostThreads > 0 ? cfg_.hostThreads : omp_get_max_threads(); }
+
 vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads,
                                   uint64_t protectTick) {
     const size_t n = bricks.size();
@@ -141,8 +143,7 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
         hostTick_[hs] = ++tick_;
         hslot[miss[k]] = hs;
     }
-    const int nth = cfg_.hostThreads;
-#pragma omp parallel for schedule(dynamic, 8) num_threads(nth > 0 ? nth : omp_get_max_threads())
+#pragma omp parallel for schedule(dynamic, 8) num_threads(host_threads())
     for (long long k = 0; k < (long long)want; k++) {
         size_t i = miss[k];
         read_brick(bricks[i], h_tier_ + (size_t)hslot[i] * slotBytes_);

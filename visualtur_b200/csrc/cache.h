@@ -50,6 +50,8 @@ public:
      * while a frame's kernels are in flight) and the device fill */
     vt_status prefetch_stage(const std::vector<uint64_t>& bricks, std::vector<uint64_t>& staged,
                              std::vector<int>& hslot, bool append = false, uint64_t protectTick = 0);
+    /* threads for host-tier reads (0 in the config: all hardware threads) */
+    int host_threads() const;
     /* host-tier clock, for protecting slots staged over several calls */
     uint64_t host_tick() const { return tick_; }
     vt_status prefetch_commit(const std::vector<uint64_t>& staged, const std::vector<int>& hslot, cudaStream_t s,
