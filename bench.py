@@ -362,6 +362,18 @@ def roofline(stats_frames, trace_ms, pixels, traffic_per_ray=None, esize=4):
             "kernel": "k_trace"}
 
 
+def hint_use(P, conf):
+    """How the timed run uses the learned prefetcher: a network is trained
+    for every out-of-core workload, and the paging tuner decides whether its
+    hints are sent (threshold) or not."""
+    if P is None:
+        return "off"
+    thr = conf.get("hint_threshold")
+    if thr is None:
+        return "trained; hints off (tuner's choice)" if "hint_threshold" in conf else "trained; no hints on batched views"
+    return "hints on (threshold %g)" % thr
+
+
 def sample_camera(cfg, step):
     """The camera the CPU baseline renders for `step`: the frame's camera,
     or the first view of a batched step."""
@@ -732,6 +744,10 @@ def run_ours(args, cfg, rank, world, torch, dist):
     tot_ms = sum(ms)
     st = wl.r.stats()
     ld = frame_deltas(per)
+    slow = sorted(range(len(per)), key=lambda k: -per[k]["ms_last_frame"])[:3]
+    log("timed: slowest launches (index: host ms, stall ms, trace ms, device ms) " + ", ".join(
+        "%d: %.2f %.2f %.2f %.2f" % (k, per[k]["ms_last_frame"], per[k]["ms_stall_last_frame"],
+                                     per[k]["ms_trace_last_frame"], ms[k]) for k in slow))
     trace_tot = sum(s["ms_trace_last_frame"] for s in per)
     rays_rank = sum(L.rays(cams) for _, _, cams, _ in launches)
     t_max = max_over_ranks(dist, torch, tot_ms, dev)
@@ -807,7 +823,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
         "vs_baseline": None, "dtype": "u8" if wl.esize == 1 else "f32",
         "data": "synthetic (seeded generators, device-generated)",
         "config": dict(conf, workload=cfg["workload"], name=args.config, mode=args.mode,
-                       learned_prefetch=P is not None, brick=wl.brick, **{
+                       learned_prefetch=hint_use(P, conf), brick=wl.brick, **{
                    "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
                    "parallelism": "replicas" if world > 1 else "single GPU"}),
         "roofline": roofline(ld, trace_tot, rays_rank, TRAFFIC_BYTES_PER_RAY.get(args.config), wl.esize),
@@ -824,6 +840,10 @@ def run_ours(args, cfg, rank, world, torch, dist):
                         "bricks_requested": st["bricks_requested"], "bricks_loaded": st["bricks_loaded_disk"],
                         "bricks_prefetched": st["bricks_prefetched"], "bricks_hinted": st["bricks_hinted"],
                         "bricks_staged": st["bricks_staged"],
+                        "bricks_speculative": st["bricks_speculative"],
+                        "first_launch_stall_ms": round(per[0]["ms_stall_last_frame"], 3),
+                        "host_read_ms_total": round(st["ms_host_read_total"], 2),
+                        "fill_wait_ms_total": round(st["ms_fill_wait_total"], 2),
                         "hits": st["hits"], "samples": st["samples"], "candidates": st["candidates"],
                         "expansions": st["expansions"]},
     }
@@ -843,6 +863,10 @@ def run_ours(args, cfg, rank, world, torch, dist):
     if not args.no_cpu_baseline:
         cb = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, step=frame0 + args.warmup)
         cb.pop("per_ray_s")
+        one = cpu_baseline(cfg, wl, wl.octree_path, max(1.0, args.cpu_budget / 3), nthreads=1,
+                           step=frame0 + args.warmup)
+        cb["value_1thread"] = one["value"]
+        cb["sample_1thread"] = one["sample"]
         line["cpu_baseline"] = cb
     return line
 

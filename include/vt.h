@@ -274,6 +274,8 @@ typedef struct {
     double  ms_last_frame, ms_stall_last_frame, bytes_h2d_last_frame;
     double  ms_trace_last_frame;    /* device time of the trace kernels of the last frame */
     double  ms_prefetch_last_frame; /* host time of the hinted prefetch's device fill */
+    double  ms_host_read_total;     /* cumulative host time reading bricks into the host tier */
+    double  ms_fill_wait_total;     /* cumulative host time waiting for device fills to finish */
 } vt_stats;
 vt_status vt_get_stats(vt_handle* h, vt_stats* s);
 /* Empties the brick cache (both tiers): the next frame starts cold.

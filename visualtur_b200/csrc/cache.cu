@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <numeric>
 
 #include <omp.h>
@@ -143,13 +144,33 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
         hostTick_[hs] = ++tick_;
         hslot[miss[k]] = hs;
     }
-#pragma omp parallel for schedule(dynamic, 8) num_threads(host_threads())
-    for (long long k = 0; k < (long long)want; k++) {
-        size_t i = miss[k];
-        read_brick(bricks[i], h_tier_ + (size_t)hslot[i] * slotBytes_);
+    const auto tr = std::chrono::steady_clock::now();
+    /* each brick is gathered in a per-thread buffer that stays in cache, then
+     * streamed to its tier slot: the tier's lines are written without being
+     * read first, and do not displace the volume rows other reads share */
+#pragma omp parallel num_threads(host_threads())
+    {
+        static thread_local std::vector<unsigned char> stage;
+        if (stage.size() < slotBytes_) stage.resize(slotBytes_);
+#pragma omp for schedule(dynamic, 8)
+        for (long long k = 0; k < (long long)want; k++) {
+            size_t i = miss[k];
+            read_brick(bricks[i], stage.data());
+            stream_copy(h_tier_ + (size_t)hslot[i] * slotBytes_, stage.data(), slotBytes_);
+        }
+        stream_fence();
     }
+    msHostRead_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tr).count();
     hostMisses_ += (int64_t)want;
     *diskLoads += (int64_t)want;
+    return VT_OK;
+}
+
+vt_status BrickCache::refresh_stamps(cudaStream_t s) {
+    if (stampsFresh_) return VT_OK;
+    CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    stampsFresh_ = true;
     return VT_OK;
 }
 
@@ -159,7 +180,12 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
     if (n == 0) return VT_OK;
     Xfer& X = xf_[xfNext_];
     xfNext_ ^= 1;
-    if (X.pending) { CKC(cudaEventSynchronize(X.ev)); X.pending = false; }
+    if (X.pending) {
+        const auto tw = std::chrono::steady_clock::now();
+        CKC(cudaEventSynchronize(X.ev));
+        X.pending = false;
+        msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
+    }
     /* bricks with a host-tier copy, at most one per device slot */
     size_t m = 0;
     while (m < n && m < (size_t)nSlots_ && hslot[m] >= 0) m++;
@@ -171,8 +197,8 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
     order.reserve(m);
     while (order.size() < m && !freeSlots_.empty()) { order.push_back(freeSlots_.back()); freeSlots_.pop_back(); }
     if (order.size() < m) {
-        CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
-        CKC(cudaStreamSynchronize(s));
+        vt_status st = refresh_stamps(s);
+        if (st != VT_OK) return st;
         ++epoch_;
         for (int round = 0; round < 2 && order.size() < m; round++) {
             const unsigned int lim = round == 0 ? std::min(frameStart_, protectFrom) : protectFrom;
@@ -240,8 +266,10 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
     CKC(cudaEventRecord(X.ev, s));
     X.pending = true;
     if (sync) {
+        const auto tw = std::chrono::steady_clock::now();
         CKC(cudaStreamSynchronize(s));
         xf_[0].pending = xf_[1].pending = false;
+        msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
     }
     *h2d += (double)np * (double)slotBytes_;
     *loaded += (int64_t)np;
@@ -256,7 +284,11 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
         CKC(cudaHostAlloc((void**)&h_req_, reqCap_ * 8, cudaHostAllocDefault));
     }
     CKC(cudaMemcpyAsync(h_req_, d_req, (size_t)nReq * 8, cudaMemcpyDeviceToHost, s));
+    /* the pass's slot stamps come with the request list, so victim choice
+     * never waits for a fill in flight */
+    if (!stampsFresh_) CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
     CKC(cudaStreamSynchronize(s));
+    stampsFresh_ = true;
     requested_ += nReq;
     std::vector<uint64_t> demand, spec;
     demand.reserve(nReq);
@@ -266,17 +298,23 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
         else demand.push_back(r);
     }
     speculative_ += (int64_t)spec.size();
+    /* in page order (z fastest): neighbouring bricks share the volume rows
+     * of their aprons, so reading them one after another hits the cache */
+    std::sort(demand.begin(), demand.end());
+    std::sort(spec.begin(), spec.end());
     int64_t disk = 0, loaded = 0;
     vt_status st;
+    const size_t kChunk = 8192;
+    /* host slots touched in this service stay put until it returns: fills of
+     * earlier chunks may still be reading them */
+    const uint64_t svcStart = tick_ + 1;
     /* demand requests first: no kernel runs, so any slot may be reused;
      * bricks over the admission cap are re-requested next pass
      * (assign_device loads the first `cap` and resets the rest) */
     if (!demand.empty()) {
         /* in chunks: the host-tier reads of one chunk overlap the device fill
-         * of the one before; host slots filled in this service stay put */
-        const size_t kChunk = 8192;
+         * of the one before */
         const size_t cap = std::min<size_t>({demand.size(), (size_t)nSlots_, (size_t)nHost_});
-        const uint64_t svcStart = tick_ + 1;
         for (size_t c0 = 0; c0 < cap; c0 += kChunk) {
             const size_t c1 = std::min(cap, c0 + kChunk);
             const bool last = c1 == cap;
@@ -285,7 +323,7 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
             if ((st = ensure_host(head, hs, &disk, svcStart)) != VT_OK) return st;
             if (last) head.insert(head.end(), demand.begin() + cap, demand.end());   /* reset to absent */
             hs.resize(head.size(), -1);
-            if ((st = assign_device(head, hs, s, 0xFFFFFFFFu, h2dBytes, &loaded, last)) != VT_OK) return st;
+            if ((st = assign_device(head, hs, s, 0xFFFFFFFFu, h2dBytes, &loaded, false)) != VT_OK) return st;
         }
     }
     /* speculative requests (lookahead): only into free slots or slots this
@@ -299,17 +337,31 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
         if (!want.empty()) {
             /* admit only as many as there are slots they may take, so no
              * host-tier read is spent on a brick that finds no slot */
-            CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
-            CKC(cudaStreamSynchronize(s));
             size_t avail = 0;
             for (int i = 0; i < nSlots_; i++) avail += slotBrick_[i] == kEmpty || stampHost_[i] < frameStart_;
-            const size_t cap = std::min<size_t>({want.size(), avail, (size_t)nHost_});
-            std::vector<uint64_t> head(want.begin(), want.begin() + cap);
-            std::vector<int> hs;
-            if ((st = ensure_host(head, hs, &disk)) != VT_OK) return st;
-            hs.resize(want.size(), -1);
-            if ((st = assign_device(want, hs, s, frameStart_, h2dBytes, &loaded)) != VT_OK) return st;
+            const size_t hostFree = (size_t)nHost_ - std::min<size_t>((size_t)nHost_, (size_t)(tick_ + 1 - svcStart));
+            const size_t cap = std::min<size_t>({want.size(), avail, hostFree});
+            /* chunked like the demand requests; slots filled by one chunk
+             * carry the current pass's stamp, so later chunks skip them */
+            for (size_t c0 = 0; c0 < cap || c0 == 0; c0 += kChunk) {
+                const size_t c1 = std::min(cap, c0 + kChunk);
+                const bool last = c1 == cap;
+                std::vector<uint64_t> head(want.begin() + c0, want.begin() + c1);
+                std::vector<int> hs;
+                if ((st = ensure_host(head, hs, &disk, svcStart)) != VT_OK) return st;
+                if (last) head.insert(head.end(), want.begin() + cap, want.end());   /* reset to absent */
+                hs.resize(head.size(), -1);
+                if ((st = assign_device(head, hs, s, frameStart_, h2dBytes, &loaded, false)) != VT_OK) return st;
+                if (last) break;
+            }
         }
+    }
+    /* fills end before the service returns (their time is a stall) */
+    if (xf_[0].pending || xf_[1].pending) {
+        const auto tw = std::chrono::steady_clock::now();
+        CKC(cudaStreamSynchronize(s));
+        xf_[0].pending = xf_[1].pending = false;
+        msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
     }
     return VT_OK;
 }
@@ -386,6 +438,7 @@ void BrickCache::fold_stats(vt_stats& st) {
     st.bricks_requested = requested_; st.bricks_loaded_disk = hostMisses_;
     st.bricks_loaded_host = hostHits_; st.bricks_prefetched = prefetched_;
     st.bricks_hinted = hinted_; st.bricks_staged = staged_; st.bricks_speculative = speculative_;
+    st.ms_host_read_total = msHostRead_; st.ms_fill_wait_total = msFillWait_;
     st.launches += launches_ - launchesFolded_;
     launchesFolded_ = launches_;
 }
@@ -398,6 +451,7 @@ vt_status BrickCache::drop() {
     for (int i = 0; i < nSlots_; i++) freeSlots_[i] = nSlots_ - 1 - i;
     clock_ = 0;
     std::fill(stampHost_.begin(), stampHost_.end(), 0);
+    stampsFresh_ = false;
     std::fill(pageMirror_.begin(), pageMirror_.end(), -1);
     std::fill(hostIndex_.begin(), hostIndex_.end(), -1);
     std::fill(hostBrick_.begin(), hostBrick_.end(), kEmpty);
@@ -409,6 +463,9 @@ vt_status BrickCache::drop() {
     return VT_OK;
 }
 
-void BrickCache::reset_stats() { hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = speculative_ = 0; }
+void BrickCache::reset_stats() {
+    hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = speculative_ = 0;
+    msHostRead_ = msFillWait_ = 0;
+}
 
 }  // namespace vtrt

@@ -39,7 +39,8 @@ public:
     vt_status preload(const std::vector<uint64_t>& bricks);
     bool all_resident() const { return allResident_; }
     void fill_args(DevBricks& b) const;
-    unsigned int next_pass() { return ++pass_; }
+    /* a kernel pass is about to stamp slots: the host's stamp copy is stale */
+    unsigned int next_pass() { stampsFresh_ = false; return ++pass_; }
     void begin_frame() { frameStart_ = pass_ + 1; }
     /* services the nReq brick requests of the last pass (d_req, device) */
     vt_status service(const unsigned long long* d_req, unsigned int nReq, cudaStream_t s, double* h2dBytes);
@@ -90,6 +91,10 @@ private:
     unsigned int epoch_ = 0;
     std::vector<int> pageMirror_;            /* host copy of page (>= 0 or -1) */
     std::vector<unsigned int> stampHost_;
+    /* stampHost_ equals the device stamps: no kernel pass ran since the copy
+     * (assign_device mirrors its own stamp writes) */
+    bool stampsFresh_ = false;
+    vt_status refresh_stamps(cudaStream_t s);
     /* host tier */
     unsigned char* h_tier_ = nullptr; void* d_tier_ = nullptr; int nHost_ = 0;
     std::vector<int> hostIndex_;             /* brick -> host slot or -1 */
@@ -112,6 +117,7 @@ private:
     int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0, hinted_ = 0, staged_ = 0,
             speculative_ = 0;
     int64_t launches_ = 0, launchesFolded_ = 0;
+    double msHostRead_ = 0, msFillWait_ = 0;
 };
 
 }  // namespace vtrt

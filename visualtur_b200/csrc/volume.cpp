@@ -15,6 +15,10 @@
 #include <cmath>
 #include <string>
 
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
+
 #include "vt_runtime.h"
 
 namespace vtrt {
@@ -84,6 +88,18 @@ static void read_box(const vt_volume* v, const int s[3], const int e[3], OutT* o
 }
 
 void volume_read(const vt_volume* v, const int s[3], const int e[3], float* out) { read_box(v, s, e, out); }
+
+#if defined(__x86_64__)
+void stream_copy(void* dst, const void* src, size_t bytes) {
+    __m128i* d = (__m128i*)dst;
+    const __m128i* q = (const __m128i*)src;
+    for (size_t i = 0; i < bytes / 16; i++) _mm_stream_si128(d + i, _mm_loadu_si128(q + i));
+}
+void stream_fence() { _mm_sfence(); }
+#else
+void stream_copy(void* dst, const void* src, size_t bytes) { memcpy(dst, src, bytes); }
+void stream_fence() {}
+#endif
 void volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out) {
     if (v->vtype == VT_F32) read_box(v, s, e, (float*)out);
     else read_box(v, s, e, (uint8_t*)out);

@@ -53,6 +53,11 @@ namespace vtrt {
 void volume_read(const vt_volume* v, const int s[3], const int e[3], float* out);
 /* same, native voxel type, into a buffer of (e-s) voxels */
 void volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out);
+/* copies `bytes` (a multiple of 16) to a 16-byte aligned `dst` with stores
+ * that bypass the caches (the destination is not read first); the calling
+ * thread ends its run of such copies with stream_fence() */
+void stream_copy(void* dst, const void* src, size_t bytes);
+void stream_fence();
 /* reference device-variant child membership (src/Octree.cu:375-532) */
 int children_mask(const uint64_t* e, int size, uint64_t father);
 /* reference host-variant child count (src/CreateOctree.cu:247-284) */
