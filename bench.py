@@ -136,12 +136,20 @@ class Clocks:
         self.p = None
 
     def start(self):
+        """Starts sampling and returns once the first sample is written:
+        nvidia-smi's start-up takes driver locks that stall CUDA calls of
+        this process for tens to hundreds of ms, which must not fall into
+        the timed region."""
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return
+        t_end = time.time() + 3.0
+        while time.time() < t_end and self.p.poll() is None and os.path.getsize(self.f.name) == 0:
+            time.sleep(0.01)
 
     def stop(self):
         if self.p is None:
@@ -745,9 +753,10 @@ def run_ours(args, cfg, rank, world, torch, dist):
     st = wl.r.stats()
     ld = frame_deltas(per)
     slow = sorted(range(len(per)), key=lambda k: -per[k]["ms_last_frame"])[:3]
-    log("timed: slowest launches (index: host ms, stall ms, trace ms, device ms) " + ", ".join(
-        "%d: %.2f %.2f %.2f %.2f" % (k, per[k]["ms_last_frame"], per[k]["ms_stall_last_frame"],
-                                     per[k]["ms_trace_last_frame"], ms[k]) for k in slow))
+    log("timed: slowest launches (index: host ms, stall ms, wait ms, trace ms, device ms) " + ", ".join(
+        "%d: %.2f %.2f %.2f %.2f %.2f" % (k, per[k]["ms_last_frame"], per[k]["ms_stall_last_frame"],
+                                          per[k]["ms_wait_last_frame"], per[k]["ms_trace_last_frame"], ms[k])
+        for k in slow))
     trace_tot = sum(s["ms_trace_last_frame"] for s in per)
     rays_rank = sum(L.rays(cams) for _, _, cams, _ in launches)
     t_max = max_over_ranks(dist, torch, tot_ms, dev)

@@ -276,6 +276,7 @@ typedef struct {
     double  ms_prefetch_last_frame; /* host time of the hinted prefetch's device fill */
     double  ms_host_read_total;     /* cumulative host time reading bricks into the host tier */
     double  ms_fill_wait_total;     /* cumulative host time waiting for device fills to finish */
+    double  ms_wait_last_frame;     /* host time of the last frame blocked on its passes' results */
 } vt_stats;
 vt_status vt_get_stats(vt_handle* h, vt_stats* s);
 /* Empties the brick cache (both tiers): the next frame starts cold.

@@ -57,7 +57,7 @@ class vt_stats(C.Structure):
         "bricks_hinted", "bricks_staged", "bricks_speculative")] + \
         [(n, C.c_double) for n in ("ms_last_frame", "ms_stall_last_frame", "bytes_h2d_last_frame",
                                    "ms_trace_last_frame", "ms_prefetch_last_frame", "ms_host_read_total",
-                                   "ms_fill_wait_total")]
+                                   "ms_fill_wait_total", "ms_wait_last_frame")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

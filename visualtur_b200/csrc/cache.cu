@@ -248,10 +248,26 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
     /* requests that got no slot go back to absent (retried next pass) */
     for (size_t k = np; k < n; k++)
         if (pageMirror_[bricks[k] - pageBase_] < 0) h_upd_[nu++] = make_int2((int)(bricks[k] - pageBase_), -1);
-    if (np) {
+    /* runs of consecutive host slots going to consecutive device slots (a
+     * cold start hands out both in order) move by the copy engine, which
+     * outruns SM loads from mapped memory over PCIe; the rest by the kernel */
+    const size_t kMinRun = 16;
+    size_t nk = 0;
+    for (size_t k = 0; k < np;) {
+        size_t e = k + 1;
+        while (e < np && h_pairs_[e].x == h_pairs_[e - 1].x + 1 && h_pairs_[e].y == h_pairs_[e - 1].y + 1) e++;
+        if (e - k >= kMinRun) {
+            CKC(cudaMemcpyAsync((unsigned char*)d_slab_ + (size_t)h_pairs_[k].y * slotBytes_, h_tier_ + (size_t)h_pairs_[k].x * slotBytes_,
+                                (e - k) * slotBytes_, cudaMemcpyHostToDevice, s));
+        } else {
+            for (size_t j = k; j < e; j++) h_pairs_[nk++] = h_pairs_[j];
+        }
+        k = e;
+    }
+    if (nk) {
         launches_++;
-        CKC(cudaMemcpyAsync(X.dp, h_pairs_, np * sizeof(int2), cudaMemcpyHostToDevice, s));
-        k_fill_bricks<<<(unsigned int)np, 256, 0, s>>>((const unsigned char*)d_tier_, slotBytes_, X.dp,
+        CKC(cudaMemcpyAsync(X.dp, h_pairs_, nk * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_fill_bricks<<<(unsigned int)nk, 256, 0, s>>>((const unsigned char*)d_tier_, slotBytes_, X.dp,
                                                        (unsigned char*)d_slab_);
         CKC(cudaGetLastError());
     }

@@ -632,7 +632,7 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
     CK(cudaEventRecord(h->ev[1], s));
     h->stats.launches++;
     int passes = 1;
-    double stall = 0, h2d = 0;
+    double stall = 0, h2d = 0, wait = 0;
     /* prefetch hint for the next frame: host-tier loads overlap this frame's kernel */
     std::vector<uint64_t> staged;
     std::vector<int> stagedSlots;
@@ -654,7 +654,9 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
         int cur = 0;
         for (;;) {
             CK(cudaMemcpyAsync(&h->h_ctl->n_out, &h->d_ctl->n_out, 8, cudaMemcpyDeviceToHost, s));
+            const auto tw = std::chrono::steady_clock::now();
             CK(cudaStreamSynchronize(s));
+            wait += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
             unsigned int nOut = h->h_ctl->n_out, nReq = h->h_ctl->n_req;
             if (nOut == 0) break;
             if (nOut > h->susp_cap) return fail(VT_ERR_STATE, "suspended-ray list overflow");
@@ -697,6 +699,7 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
     h->stats.frames++;
     h->stats.passes = passes;
     h->stats.ms_stall_last_frame = stall;
+    h->stats.ms_wait_last_frame = wait;
     h->stats.bytes_h2d_last_frame = h2d;
     if (h->cache) h->cache->fold_stats(h->stats);
     h->stats.ms_last_frame = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
