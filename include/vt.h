@@ -261,6 +261,14 @@ vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n);
  * code at levelCubes, hit distance along the ray, unit normal. */
 vt_status vt_debug_hits(vt_handle* h, uint64_t* node_id, uint64_t* brick_id, float* t, float* normal);
 
+/* Copies the device-cache slot of brick `code` (Morton code at levelCubes)
+ * into host_out: (edge + 2*cubeInc)^3 voxels of the volume's type, the
+ * zero-padded box [min - cubeInc, min + edge + cubeInc) x slowest, as
+ * lruCache's bricks (src/lruCache.cu:224-226).  *resident = 0, and nothing
+ * is copied, when the brick has no slot (or the renderer is resident).
+ * Synchronises the device. */
+vt_status vt_debug_slot(vt_handle* h, uint64_t code, void* host_out, int* resident);
+
 typedef struct {
     int64_t frames, rays, hits, samples, normal_samples, candidates, expansions;
     int64_t passes;                 /* demand passes in the last frame */

@@ -124,6 +124,7 @@ _PROTOS = {
     "vt_get_trace": (C.c_int, [_P, _P, C.c_int64]),
     "vt_prefetch": (C.c_int, [_P, _P, C.c_int64, C.POINTER(C.c_int64), _P]),
     "vt_brick_list": (C.c_int, [_P, _P, C.POINTER(C.c_int64)]),
+    "vt_debug_slot": (C.c_int, [_P, C.c_uint64, _P, C.POINTER(C.c_int)]),
     "vt_prefetch_hint": (C.c_int, [_P, _P, C.c_int64]),
     "vt_set_tuning": (C.c_int, [_P, C.POINTER(vt_tuning)]),
     "vt_drop_cache": (C.c_int, [_P]),
@@ -502,6 +503,14 @@ class visualTur:
         out = np.empty(n.value, np.uint64)
         check(lib().vt_brick_list(self._h, out.ctypes.data, C.byref(n)))
         return out
+
+    def debug_slot(self, code, D, dtype):
+        """The device-cache slot of brick `code` as a D x D x D array of
+        `dtype`, or None when the brick has no slot."""
+        out = np.empty((D, D, D), dtype)
+        res = C.c_int(0)
+        check(lib().vt_debug_slot(self._h, int(code), out.ctypes.data, C.byref(res)))
+        return out if res.value else None
 
     def stats(self):
         s = vt_stats()

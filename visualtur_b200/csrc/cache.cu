@@ -479,6 +479,18 @@ vt_status BrickCache::drop() {
     return VT_OK;
 }
 
+vt_status BrickCache::copy_slot(uint64_t page, void* host, int* resident) {
+    *resident = 0;
+    if (page - pageBase_ >= pageN_) return fail(VT_ERR_INVALID, "brick outside the brick grid");
+    const int slot = pageMirror_[page - pageBase_];
+    if (slot < 0) return VT_OK;
+    CKC(cudaDeviceSynchronize());
+    CKC(cudaMemcpy(host, (unsigned char*)d_slab_ + (size_t)slot * slotBytes_, (size_t)D_ * D_ * D_ * esize_,
+                   cudaMemcpyDeviceToHost));
+    *resident = 1;
+    return VT_OK;
+}
+
 void BrickCache::reset_stats() {
     hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = speculative_ = 0;
     msHostRead_ = msFillWait_ = 0;

@@ -62,6 +62,8 @@ public:
     vt_status drop();
     void reset_stats();
     int device_slots() const { return nSlots_; }
+    /* host copy of a brick's device slot (D^3 voxels); *resident = 0 if none */
+    vt_status copy_slot(uint64_t page, void* host, int* resident);
     size_t slot_bytes() const { return slotBytes_; }
 
 private:

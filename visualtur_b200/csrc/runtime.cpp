@@ -826,6 +826,14 @@ extern "C" vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n) {
     return VT_OK;
 }
 
+extern "C" vt_status vt_debug_slot(vt_handle* h, uint64_t code, void* host_out, int* resident) {
+    clear_error();
+    if (!h || !host_out || !resident) return fail(VT_ERR_INVALID, "null argument");
+    *resident = 0;
+    if (!h->cache) return VT_OK;
+    return h->cache->copy_slot(code_to_page(code, h->Lc), host_out, resident);
+}
+
 extern "C" vt_status vt_drop_cache(vt_handle* h) {
     clear_error();
     if (!h) return fail(VT_ERR_INVALID, "null handle");
