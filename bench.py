@@ -552,9 +552,10 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
     with torch.cuda.stream(stream):
         f = frame0
         while f < frame0 + warmup:
-            n = min(L.batch, frame0 + warmup - f)
-            nxt = min(L.batch, frame0 + warmup + steps - f - n)
-            L.launch(L.cams(f, n), L.cams(f + n, nxt), f)
+            # whole launches, as timed: buffers sized by the views per launch
+            # are allocated here, not in the first timed launch
+            n = L.batch
+            L.launch(L.cams(f, n), L.cams(f + n, n), f)
             f += n
         torch.cuda.synchronize()
         if not L.cfg["resident"] and not L.warm:

@@ -215,6 +215,10 @@ static vt_status ensure_suspend_buffers(vt_handle* h, unsigned int rays) {
         cudaFree(h->d_susp[i]); cudaFree(h->d_pool[i]);
         h->d_susp[i] = nullptr; h->d_pool[i] = nullptr;
     }
+    /* grow by half again at least: a caller that adds views one at a time
+     * reallocates (and synchronises the device) only a few times */
+    rays = (unsigned int)std::min<unsigned long long>(0xFFFFFFFFull,
+                                                      std::max<unsigned long long>(rays, h->susp_cap + h->susp_cap / 2ull));
     h->susp_cap = rays;
     h->pool_cap = (unsigned long long)rays * 12ull;
     for (int i = 0; i < 2; i++) {
