@@ -148,11 +148,15 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
     /* each brick is gathered in a per-thread buffer that stays in cache, then
      * streamed to its tier slot: the tier's lines are written without being
      * read first, and do not displace the volume rows other reads share */
-#pragma omp parallel num_threads(host_threads())
+    /* a few hundred bricks (a steady-state pass) still spread over every
+     * thread */
+    const int nth = host_threads();
+    const int grain = (int)std::max<size_t>(1, std::min<size_t>(8, want / ((size_t)nth * 4)));
+#pragma omp parallel num_threads(nth)
     {
         static thread_local std::vector<unsigned char> stage;
         if (stage.size() < slotBytes_) stage.resize(slotBytes_);
-#pragma omp for schedule(dynamic, 8)
+#pragma omp for schedule(dynamic, grain)
         for (long long k = 0; k < (long long)want; k++) {
             size_t i = miss[k];
             read_brick(bricks[i], stage.data());
@@ -320,7 +324,10 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
     std::sort(spec.begin(), spec.end());
     int64_t disk = 0, loaded = 0;
     vt_status st;
-    const size_t kChunk = 8192;
+    /* chunk size: large services in chunks of 8 192 bricks; small ones (a
+     * steady-state pass) still in four, so the reads of one overlap the
+     * transfer of the one before */
+    const size_t kChunk = std::min<size_t>(8192, std::max<size_t>(64, ((size_t)nReq + 3) / 4));
     /* host slots touched in this service stay put until it returns: fills of
      * earlier chunks may still be reading them */
     const uint64_t svcStart = tick_ + 1;

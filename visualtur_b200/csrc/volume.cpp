@@ -58,9 +58,11 @@ static void read_box(const vt_volume* v, const int s[3], const int e[3], OutT* o
         if (dr[a] <= 0) return;
     }
     /* rows are short and far apart (one per y, x): fetch PF rows ahead,
-     * walking a second (x, y) cursor */
-    const int PF = 8;
+     * walking a second (x, y) cursor; rows under a cache line need more
+     * rows in flight (38^3 u8 brick boxes: 32 rows ahead ~10 % faster than
+     * 8; 22^3 f32 boxes: no gain) */
     const size_t es = v->esize(), rowBytes = (size_t)dr[2] * es;
+    const int PF = rowBytes < 64 ? 32 : 8;
     int64_t pa = 0, pb = 0;
     auto prefetch_next = [&]() {
         if (pa >= dr[0]) return;
