@@ -5,14 +5,17 @@
  * Device tier: a slab of `deviceSlots` bricks of (edge + 2*inc)^3 voxels and
  * a direct-mapped page table indexed by brick Morton code (8^levelCubes
  * entries indexed bx << 2Lc | by << Lc | bz: slot >= 0, -1 absent, -2
- * requested this pass).  Bricks are keyed by that page index throughout.  Kernels look
- * bricks up with one load and request absent ones with one atomicCAS; each
- * use stamps the slot with the pass number, and eviction between passes
- * takes the least recently used slots.
+ * requested this pass, -3 requested by a lookahead).  Bricks are keyed by
+ * that page index throughout.  Kernels look bricks up with one load and
+ * request absent ones with one atomicCAS; each use stamps the slot with the
+ * pass number, and eviction between passes takes the least recently used
+ * slots.
  * Host tier: `hostSlots` bricks in pinned, device-mapped memory with the
  * same LRU rule; misses read the brick zero-padded from the volume source
- * (FileManager::readHDF5_Voxel_Array semantics) on host threads.  A fill
- * kernel copies host-tier bricks into their device slots over PCIe/C2C.
+ * (FileManager::readHDF5_Voxel_Array semantics) on host threads.  Bricks
+ * cross to their device slots by the copy engine where consecutive host
+ * slots go to consecutive device slots, else by a fill kernel reading the
+ * mapped tier.
  */
 #pragma once
 #include <cuda_runtime.h>
