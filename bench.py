@@ -639,20 +639,23 @@ def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=Fa
     return Launcher(wl, r, cfg, torch, dev, stream, batch=batch, predictor=predictor, warm=warm)
 
 
-PAGING_CANDIDATES = ((8, 2), (4, 2), (2, 2), (1, 2), (1, 0))   # (frames per launch, lookahead)
+# (frames per launch, lookahead, absent-brick candidates a ray may set aside)
+PAGING_CANDIDATES = ((8, 2, 0), (4, 2, 0), (2, 2, 0), (1, 2, 0), (1, 0, 0),
+                     (4, 2, 4), (2, 2, 4), (4, 0, 4), (2, 0, 4), (1, 0, 4))
 HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
 
 
 def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
-    """Frames per launch, lookahead and the prefetch-hint threshold for an
-    out-of-core fly-through: each candidate renders the same `frames`
+    """Frames per launch, lookahead, absent-brick candidates set aside per
+    pass and the prefetch-hint threshold for an out-of-core fly-through:
+    each candidate renders the same `frames`
     frames (another stretch of the path than the timed one) from a cold
     cache; the fastest total device time wins.  Batching more frames per
     launch amortises launches and host work but needs their joint working
     set in the device cache, and hints help only while the cache has room
     for them -- a small cache thrashes, which only a cold-cache run shows."""
-    def run(b, la, thr):
-        wl.r.set_tuning(lookahead=la)
+    def run(b, la, thr, sk=0):
+        wl.r.set_tuning(lookahead=la, skip=sk)
         L = make_launcher(wl, wl.r, cfg, torch, dev, stream, b, predictor=P)
         L.thr = thr
         wl.r.drop_cache()
@@ -667,16 +670,20 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
             e.record(stream)
             torch.cuda.synchronize()
         ms = a.elapsed_time(e)
-        log("autotune: %d frames/launch, lookahead %d, hints %s -> %.1f ms for %d frames" % (b, la, thr, ms, frames))
-        return {"frames_per_launch": b, "lookahead": la, "hint_threshold": thr, "ms": round(ms, 2)}
+        log("autotune: %d frames/launch, lookahead %d, hints %s, skip %d -> %.1f ms for %d frames" %
+            (b, la, thr, sk, ms, frames))
+        return {"frames_per_launch": b, "lookahead": la, "hint_threshold": thr, "skip": sk, "ms": round(ms, 2)}
 
     thr0 = 0.5 if P is not None else None
-    rows = [run(b, la, thr0) for b, la in PAGING_CANDIDATES]
+    rows = [run(b, la, thr0, sk) for b, la, sk in PAGING_CANDIDATES]
     best = min(rows, key=lambda x: x["ms"])
     if P is not None:
-        rows += [run(best["frames_per_launch"], best["lookahead"], t) for t in HINT_THRESHOLDS]
+        rows += [run(best["frames_per_launch"], best["lookahead"], t, best["skip"]) for t in HINT_THRESHOLDS]
         best = min(rows, key=lambda x: x["ms"])
-    wl.r.set_tuning(lookahead=best["lookahead"])
+    if best["skip"]:
+        rows.append(run(best["frames_per_launch"], best["lookahead"], best["hint_threshold"], 2))
+        best = min(rows, key=lambda x: x["ms"])
+    wl.r.set_tuning(lookahead=best["lookahead"], skip=best["skip"])
     wl.r.drop_cache()
     return best, rows
 
@@ -732,8 +739,9 @@ def run_ours(args, cfg, rank, world, torch, dist):
     if args.paging and not cfg["resident"] and "views" not in cfg:
         v = args.paging.split(",")
         fixed = {"frames_per_launch": int(v[0]), "lookahead": int(v[1]),
-                 "hint_threshold": float(v[2]) if len(v) > 2 and v[2] not in ("", "none") else None}
-        wl.r.set_tuning(lookahead=fixed["lookahead"])
+                 "hint_threshold": float(v[2]) if len(v) > 2 and v[2] not in ("", "none") else None,
+                 "skip": int(v[3]) if len(v) > 3 else 0}
+        wl.r.set_tuning(lookahead=fixed["lookahead"], skip=fixed["skip"])
         batch = fixed["frames_per_launch"]
         paging = {"best": fixed, "table": []}
     elif M["autotune"] and not args.no_autotune and not cfg["resident"] and "views" not in cfg:
@@ -741,8 +749,12 @@ def run_ours(args, cfg, rank, world, torch, dist):
         paging, prow = tune_paging(wl, cfg, torch, dev, stream, P, frame0 + args.warmup + args.steps + 97)
         batch = paging["frames_per_launch"]
         paging = {"best": paging, "table": prow}
+    if args.skip is not None:
+        wl.r.set_tuning(skip=args.skip)
     if M["autotune"] and not args.no_autotune:
         tune = autotune(args, wl, cfg, torch, dev, stream, frame0, batch)
+        if args.skip is not None:      # the brick sweep may have built a new renderer
+            wl.r.set_tuning(skip=args.skip)
     if P is not None:
         P.set_bricks(wl.r.brick_list(), wl.oc.nLevels - int(round(math.log2(wl.brick))))
     L = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch, predictor=P, warm=args.warm)
@@ -820,7 +832,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
         conf = {"views_per_launch": cfg["views"]["n"], "resolutions": [list(r) for r in cfg["views"]["res"]],
                 "rays_per_step": round(rays_rank / args.steps)}
     else:
-        conf = {"W": W, "H": H, "frames_per_launch": batch}
+        conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": wl.r.tuning()["skip"]}
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
@@ -936,9 +948,12 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="best mode without the learned prefetch")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-brick-sweep", action="store_true", help="batched configs: keep the config's brick size")
-    ap.add_argument("--paging", default=None, help="fly-throughs: fixed FRAMES,LOOKAHEAD[,HINT_THRESHOLD] instead of "
-                                                   "the paging autotune")
+    ap.add_argument("--paging", default=None, help="fly-throughs: fixed FRAMES,LOOKAHEAD[,HINT_THRESHOLD[,SKIP]] "
+                                                   "instead of the paging autotune")
     ap.add_argument("--warm", action="store_true", help="profiling: preloaded cache, no cold start")
+    ap.add_argument("--skip", type=int, default=None,
+                    help="absent-brick candidates a ray may set aside per pass (default: tuned on fly-throughs, 0 on "
+                         "batched views)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -188,6 +188,11 @@ typedef struct {
                               reference (src/rayCaster.cu:227-228); k in 1..16 = k
                               bisection steps on the bracketing samples, then the
                               linear step.  Node and brick ids do not depend on it. */
+    int skip;              /* 0..4: candidates whose brick is absent a ray may set aside
+                              (requesting the brick) to march later ones in the same
+                              pass; a hit found past them waits for them, so the image
+                              is the in-order one.  0 = stop at the first absent brick,
+                              as the reference.  Off while record_trace is on. */
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -213,9 +218,10 @@ vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], i
 
 /* Kernel schedule knobs of a live handle (autotuner): ray-tile shape,
  * march unroll, persistent ray queue, traversal steps between refills,
- * persistent CTAs per SM, lookahead requests, graph replay. */
+ * persistent CTAs per SM, lookahead requests, graph replay, absent-brick
+ * candidates set aside per pass. */
 typedef struct {
-    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph;
+    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip;
 } vt_tuning;
 vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t);
 vt_status vt_get_tuning(vt_handle* h, vt_tuning* t);

@@ -40,6 +40,7 @@ def test_chunked_service_matches_resident(cuda):
 
     res = make(1)
     dem = make(0, lookahead=4)
+    skp = make(0, skip=4, persistent=1)      # candidates behind absent bricks marched in the same pass
     c = (N - 1) / 2.0
     first = None
     for f in range(3):
@@ -48,12 +49,16 @@ def test_chunked_service_matches_resident(cuda):
                          (c, c, c))
         res.set_camera(cam)
         dem.set_camera(cam)
+        skp.set_camera(cam)
         ra, _ = res.render_host(rgb8=False)
         da, _ = dem.render_host(rgb8=False)
+        sa, _ = skp.render_host(rgb8=False)
         st = dem.stats()
         if first is None:
             first = st["bricks_requested"]
         assert np.array_equal(ra.view(np.uint32), da.view(np.uint32)), "frame %d differs" % f
+        assert np.array_equal(ra.view(np.uint32), sa.view(np.uint32)), "frame %d differs (skip)" % f
     assert first > 8192, "first pass requested only %d bricks" % first
     res.close()
     dem.close()
+    skp.close()

@@ -152,6 +152,7 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
 /* Stack entry: (node index in its level << code_bits) | Morton code. */
 struct Stk {
     unsigned long long e[VT_STACK];
+    unsigned long long sk[VT_SKIP_MAX];   /* passed-over candidates, DFS order */
 };
 
 /* stack entry helpers (layout in vt_kernels.h) */
@@ -205,9 +206,16 @@ struct Ray {
     float t;
     float3 n;
     bool hit;
+    int nskip;             /* candidates passed over (brick absent), in st.sk */
+    bool tent;             /* the pixel holds a hit found past them */
+    bool resumeSkips;      /* the passed-over candidates come first (a resumed ray) */
 };
 
-enum { RAY_RUNNING = 0, RAY_DONE = 1, RAY_SUSPENDED = 2 };
+/* RAY_TENTATIVE: a hit past passed-over candidates (the pixel is written,
+ * the ray suspends until they are decided); RAY_DONE_WRITTEN: they all
+ * missed, the pixel written earlier stands. */
+enum { RAY_RUNNING = 0, RAY_DONE = 1, RAY_SUSPENDED = 2, RAY_TENTATIVE = 3, RAY_DONE_WRITTEN = 4 };
+enum { CAND_MISSING = 0, CAND_EMPTY = 1, CAND_HIT = 2 };
 
 /* Requests page `pidx` once per pass.  A demand request (a ray waits on
  * the brick) moves the page from absent (-1) or speculatively requested
@@ -365,21 +373,93 @@ __device__ __forceinline__ bool expand(const TraceArgs& A, const RayInv& r, Stk&
     return true;
 }
 
-/* Advances one ray's DFS by at most `budget` steps (src/Octree.cu:620-720
- * interleaved with src/rayCaster.cu:139-265): inner nodes are expanded
- * until a candidate is on top, then the candidate is marched.  Returns
- * RAY_DONE when the ray is shaded or exhausted, RAY_SUSPENDED when its next
- * candidate's brick is not resident (the candidate stays on the stack),
- * RAY_RUNNING when the budget ran out. */
+/* Candidate `ent` (a node at octreeLevel): brick lookup
+ * (lruCache::updateCube, src/lruCache.cu:177-291), then march and shade
+ * (src/rayCaster.cu:139-265).  CAND_MISSING when the brick is absent (it is
+ * requested), CAND_HIT with R's hit fields set, else CAND_EMPTY. */
 template <int VTYPE, bool SLAB, int U>
-__device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, int budget) {
+__device__ __forceinline__ int candidate(const TraceArgs& A, Ray& R, unsigned long long ent, unsigned int* cnt) {
     const DevOctree& O = A.oct;
     const int nLevels = O.nLevels, Lo = O.Lo, Lc = O.Lc;
     const int dimO = 1 << (nLevels - Lo);
+    const unsigned int x = e_x(ent), y = e_y(ent), z = e_z(ent);
+    const unsigned int bx = x >> (Lo - Lc), by = y >> (Lo - Lc), bz = z >> (Lo - Lc);
+    const unsigned int pidx = (bx << (2 * Lc)) | (by << Lc) | bz;
+    Samp s; int slot;
+    setup_sampler<VTYPE, SLAB>(A, bx, by, bz, pidx, s, &slot);
+    if (SLAB && slot < 0) {
+        if (slot == -1 || slot == VT_PAGE_SPECULATIVE) request_brick(A, pidx);
+        cnt[VT_C_DEVMISSES]++;
+        return CAND_MISSING;
+    }
+    cnt[VT_C_CANDIDATES]++;
+    if (SLAB) {
+        cnt[VT_C_DEVHITS]++;
+        if (slot != R.lastSlot) { A.br.stamp[slot] = A.br.pass; R.lastSlot = slot; }   /* once per brick run */
+    }
+    if (A.ctl.touched) {
+        const int d = A.ctl.touch_shift / 3;   /* Lo - trace level */
+        unsigned long long tn = (spread3(x >> d) << 2) | (spread3(y >> d) << 1) | spread3(z >> d);
+        atomicOr(&A.ctl.touched[tn >> 5], 1u << (tn & 31));
+    }
+    const int mbx = (int)(x << (nLevels - Lo)), mby = (int)(y << (nLevels - Lo)), mbz = (int)(z << (nLevels - Lo));
+    float tn, tf;
+    if (!slab(R.r, mbx, mby, mbz, mbx + dimO, mby + dimO, mbz + dimO, &tn, &tf)) return CAND_EMPTY;
+    float3 X;
+    unsigned int ns = 0;
+    bool h = march<VTYPE, SLAB, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
+    cnt[VT_C_SAMPLES] += ns;
+    if (!h) return CAND_EMPTY;
+    /* shade (src/rayCaster.cu:238-250) */
+    float3 n = normal_at<VTYPE, SLAB>(s, X);
+    cnt[VT_C_NSAMPLES] += 6;
+    float3 l = normalize(sub(X, A.light));
+    float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
+    float a = X.y / 256.0f;
+    R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
+    R.hit = true; R.node = node_code(x, y, z, Lo); R.brick = node_code(bx, by, bz, Lc); R.n = n;
+    R.t = dot(sub(X, R.r.o), R.dir);
+    return CAND_HIT;
+}
+
+/* Advances one ray's DFS by at most `budget` steps (src/Octree.cu:620-720
+ * interleaved with src/rayCaster.cu:139-265): inner nodes are expanded
+ * until a candidate is on top, then the candidate is marched.  Returns
+ * RAY_DONE when the ray is shaded or exhausted, RAY_SUSPENDED when it must
+ * wait for absent bricks, RAY_RUNNING when the budget ran out.
+ *
+ * Passing over absent bricks (A.ctl.skip > 0): a candidate whose brick is
+ * absent is requested and set aside, and the DFS goes on to later
+ * candidates, up to A.ctl.skip of them a pass.  The first hit still wins in
+ * DFS order: a hit found past set-aside candidates is tentative (written,
+ * RAY_TENTATIVE), the rest of the DFS is dropped, and the next pass marches
+ * the set-aside candidates first, in order; the first of them that hits
+ * replaces it, and if none does it stands.  So a ray whose candidates lie
+ * in several absent bricks asks for all of them in one pass instead of one
+ * per pass, and the image is the one of the in-order traversal. */
+template <int VTYPE, bool SLAB, int U>
+__device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, int budget) {
+    const int Lo = A.oct.Lo;
+    if (SLAB) {
+        while (R.resumeSkips) {
+            if (R.nskip == 0) {
+                R.resumeSkips = false;
+                if (R.tent) return RAY_DONE_WRITTEN;
+                break;
+            }
+            if (budget-- == 0) return RAY_RUNNING;
+            const int c = candidate<VTYPE, SLAB, U>(A, R, st.sk[0], cnt);
+            if (c == CAND_MISSING) return RAY_SUSPENDED;
+            for (int k = 1; k < R.nskip; k++) st.sk[k - 1] = st.sk[k];
+            R.nskip--;
+            if (c == CAND_HIT) { R.nskip = 0; R.resumeSkips = false; return RAY_DONE; }
+        }
+    }
+    const int K = (SLAB && !A.ctl.touched) ? A.ctl.skip : 0;
     for (;;) {
         unsigned long long ent;
         for (;;) {
-            if (R.top < 0) return RAY_DONE;   /* exhausted: background */
+            if (R.top < 0) return (SLAB && R.nskip > 0) ? RAY_SUSPENDED : RAY_DONE;   /* exhausted: background */
             ent = st.e[R.top];
             if (e_level(ent) == Lo) break;
             if (budget-- == 0) return RAY_RUNNING;
@@ -388,46 +468,17 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
             if (!expand(A, R.r, st, R.top, ent, cnt, true)) return RAY_DONE;
         }
         if (budget-- == 0) return RAY_RUNNING;
-        /* candidate: brick lookup (lruCache::updateCube, src/lruCache.cu:177-291) */
-        const unsigned int x = e_x(ent), y = e_y(ent), z = e_z(ent);
-        const unsigned int bx = x >> (Lo - Lc), by = y >> (Lo - Lc), bz = z >> (Lo - Lc);
-        const unsigned int pidx = (bx << (2 * Lc)) | (by << Lc) | bz;
-        Samp s; int slot;
-        setup_sampler<VTYPE, SLAB>(A, bx, by, bz, pidx, s, &slot);
-        if (SLAB && slot < 0) {
-            if (slot == -1 || slot == VT_PAGE_SPECULATIVE) request_brick(A, pidx);
-            cnt[VT_C_DEVMISSES]++;
-            return RAY_SUSPENDED;
+        const int c = candidate<VTYPE, SLAB, U>(A, R, ent, cnt);
+        if (c == CAND_MISSING) {
+            if (R.nskip < K) { st.sk[R.nskip++] = ent; R.top--; continue; }
+            return RAY_SUSPENDED;   /* the candidate stays on the stack */
         }
         R.top--;
-        cnt[VT_C_CANDIDATES]++;
-        if (SLAB) {
-            cnt[VT_C_DEVHITS]++;
-            if (slot != R.lastSlot) { A.br.stamp[slot] = A.br.pass; R.lastSlot = slot; }   /* once per brick run */
-        }
-        if (A.ctl.touched) {
-            const int d = A.ctl.touch_shift / 3;   /* Lo - trace level */
-            unsigned long long tn = (spread3(x >> d) << 2) | (spread3(y >> d) << 1) | spread3(z >> d);
-            atomicOr(&A.ctl.touched[tn >> 5], 1u << (tn & 31));
-        }
-        const int mbx = (int)(x << (nLevels - Lo)), mby = (int)(y << (nLevels - Lo)), mbz = (int)(z << (nLevels - Lo));
-        float tn, tf;
-        if (!slab(R.r, mbx, mby, mbz, mbx + dimO, mby + dimO, mbz + dimO, &tn, &tf)) continue;
-        float3 X;
-        unsigned int ns = 0;
-        bool h = march<VTYPE, SLAB, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
-        cnt[VT_C_SAMPLES] += ns;
-        if (h) {
-            /* shade (src/rayCaster.cu:238-250) */
-            float3 n = normal_at<VTYPE, SLAB>(s, X);
-            cnt[VT_C_NSAMPLES] += 6;
-            float3 l = normalize(sub(X, A.light));
-            float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
-            float a = X.y / 256.0f;
-            R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
-            R.hit = true; R.node = node_code(x, y, z, Lo); R.brick = node_code(bx, by, bz, Lc); R.n = n;
-            R.t = dot(sub(X, R.r.o), R.dir);
-            return RAY_DONE;
+        if (c == CAND_HIT) {
+            if (!SLAB || R.nskip == 0) return RAY_DONE;
+            R.top = -1;             /* later candidates cannot matter */
+            R.tent = true;
+            return RAY_TENTATIVE;
         }
     }
 }
@@ -491,9 +542,15 @@ __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, 
     R.hit = false; R.node = 0; R.brick = 0; R.t = -1.0f; R.n = f3(0, 0, 0);
     R.top = -1;
     R.lastSlot = -1;
+    R.nskip = 0; R.tent = false; R.resumeSkips = false;
     if (resume && depth > 0) {
-        R.top = (int)depth - 1;
-        for (int e = 0; e <= R.top; e++) st.e[e] = A.ctl.pool_in[off + e];
+        const int nsk = (int)((depth >> 8) & 7u);
+        R.top = (int)(depth & 255u) - 1;
+        R.nskip = nsk;
+        R.tent = (depth >> 11) & 1u;
+        R.resumeSkips = nsk > 0 || R.tent;
+        for (int e = 0; e < nsk; e++) st.sk[e] = A.ctl.pool_in[off + e];
+        for (int e = 0; e <= R.top; e++) st.e[e] = A.ctl.pool_in[off + nsk + e];
         return RAY_RUNNING;
     }
     if (!resume) cnt[VT_C_RAYS]++;
@@ -504,10 +561,12 @@ __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, 
     return RAY_DONE;   /* background */
 }
 
-__device__ __forceinline__ void write_ray(const TraceArgs& A, const DevView* sv, const Ray& R, unsigned int* cnt) {
+/* count = false: the pixel was counted when a tentative hit was written */
+__device__ __forceinline__ void write_ray(const TraceArgs& A, const DevView* sv, const Ray& R, unsigned int* cnt,
+                                          bool count = true) {
     const DevView& V = sv[R.view];
     const size_t id = (size_t)R.i * V.cam.W + R.j;
-    if (R.hit) cnt[VT_C_HITS]++;
+    if (R.hit && count) cnt[VT_C_HITS]++;
     if (V.rgba) V.rgba[id] = R.rgba;
     if (V.rgb8) {
         V.rgb8[3 * id] = to_u8(R.rgba.x);
@@ -527,13 +586,14 @@ __device__ __forceinline__ void suspend_ray(const TraceArgs& A, Ray& R, Stk& st,
     cnt[VT_C_SUSPENDED]++;
     unsigned int q = atomicAdd(A.ctl.n_out, 1u);
     if (q >= A.ctl.out_cap) { atomicOr(A.ctl.err, VT_KERR_SUSPEND_FULL); return; }
-    unsigned int depth = (unsigned int)(R.top + 1);
-    unsigned long long off = atomicAdd(A.ctl.pool_used, (unsigned long long)depth);
+    const unsigned int depth = (unsigned int)(R.top + 1), nsk = (unsigned int)R.nskip;
+    unsigned long long off = atomicAdd(A.ctl.pool_used, (unsigned long long)(depth + nsk));
     SuspRec rec;
     rec.ray = R.g;
-    if (off + depth <= A.ctl.pool_cap) {
-        for (unsigned int e = 0; e < depth; e++) A.ctl.pool_out[off + e] = st.e[e];
-        rec.depth = depth; rec.off = off;
+    if (off + depth + nsk <= A.ctl.pool_cap) {
+        for (unsigned int e = 0; e < nsk; e++) A.ctl.pool_out[off + e] = st.sk[e];
+        for (unsigned int e = 0; e < depth; e++) A.ctl.pool_out[off + nsk + e] = st.e[e];
+        rec.depth = depth | (nsk << 8) | ((R.tent ? 1u : 0u) << 11); rec.off = off;
     } else {
         rec.depth = 0; rec.off = 0;   /* pool full: the ray restarts from the root (same result) */
     }
@@ -578,7 +638,8 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
         if (w < nItems) {
             int s = start_ray<VTYPE>(A, sv, w, R, st, cnt);
             if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB, U>(A, R, st, cnt, -1);
-            if (s == RAY_DONE) write_ray(A, sv, R, cnt);
+            if (s == RAY_DONE) write_ray(A, sv, R, cnt, !R.tent);
+            else if (s == RAY_TENTATIVE) { write_ray(A, sv, R, cnt); suspend_ray<VTYPE, SLAB>(A, R, st, cnt); }
             else if (s == RAY_SUSPENDED) suspend_ray<VTYPE, SLAB>(A, R, st, cnt);
         }
     } else {
@@ -603,8 +664,13 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
             }
             if (has) {
                 int s = run_ray<VTYPE, SLAB, U>(A, R, st, cnt, A.pops);
-                if (s == RAY_DONE) { write_ray(A, sv, R, cnt); has = false; }
-                else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB>(A, R, st, cnt); has = false; }
+                if (s == RAY_DONE) { write_ray(A, sv, R, cnt, !R.tent); has = false; }
+                else if (s == RAY_TENTATIVE) {
+                    write_ray(A, sv, R, cnt);
+                    suspend_ray<VTYPE, SLAB>(A, R, st, cnt);
+                    has = false;
+                } else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB>(A, R, st, cnt); has = false; }
+                else if (s == RAY_DONE_WRITTEN) has = false;
             }
         }
     }

@@ -354,6 +354,7 @@ static vt_status validate(const vt_params* p, const vt_octree* o, const vt_optio
         if (opt->unroll != 1 && opt->unroll != 2 && opt->unroll != 4 && opt->unroll != 8)
             return fail(VT_ERR_INVALID, "unroll must be 1, 2, 4 or 8");
         if (opt->refine < 0 || opt->refine > 16) return fail(VT_ERR_INVALID, "refine must be in 0..16");
+        if (opt->skip < 0 || opt->skip > VT_SKIP_MAX) return fail(VT_ERR_INVALID, "skip must be in 0..%d", VT_SKIP_MAX);
         if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
             return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
     }
@@ -526,6 +527,7 @@ static void fill_args(vt_handle* h, TraceArgs& a, int nViews, unsigned int total
     a.ctl.n_out = &c->n_out; a.ctl.n_req = &c->n_req; a.ctl.pool_used = &c->pool_used;
     a.ctl.req = h->d_req; a.ctl.req_cap = h->req_cap;
     a.ctl.lookahead = h->opt.lookahead;
+    a.ctl.skip = h->opt.skip;
     if (h->d_touched) {
         a.ctl.touched = h->d_touched;
         a.ctl.touch_shift = 3 * (h->Lo - h->opt.trace_level);
@@ -792,6 +794,7 @@ extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
     vt_options o = h->opt;
     o.tile_w = t->tile_w; o.tile_h = t->tile_h; o.unroll = t->unroll; o.persistent = t->persistent;
     o.pops = t->pops; o.blocks_per_sm = t->blocks_per_sm; o.lookahead = t->lookahead; o.use_graph = t->use_graph;
+    o.skip = t->skip;
     vt_status s = validate(&h->p, h->oct, &o);
     if (s != VT_OK) return s;
     if (o.lookahead < 0 || o.lookahead > 64 || o.pops < 1 || o.blocks_per_sm < 1 || o.blocks_per_sm > 32)
@@ -806,6 +809,7 @@ extern "C" vt_status vt_get_tuning(vt_handle* h, vt_tuning* t) {
     t->tile_w = h->opt.tile_w; t->tile_h = h->opt.tile_h; t->unroll = h->opt.unroll; t->persistent = h->opt.persistent;
     t->pops = h->opt.pops; t->blocks_per_sm = h->opt.blocks_per_sm; t->lookahead = h->opt.lookahead;
     t->use_graph = h->opt.use_graph;
+    t->skip = h->opt.skip;
     return VT_OK;
 }
 

@@ -8,6 +8,7 @@
 
 #define VT_MAX_LEVELS 20
 #define VT_STACK 64          /* per-ray DFS stack entries (reference: 32) */
+#define VT_SKIP_MAX 4        /* absent-brick candidates a ray may pass over in one pass */
 
 /* error bits reported by kernels through DevCtl::err */
 #define VT_KERR_STACK 1u        /* a ray's stack overflowed */
@@ -86,6 +87,9 @@ struct DevViews {
 
 /* A suspended ray: padded global ray index, saved stack depth (0 = restart
  * from the root) and offset of its entries in the stack pool. */
+/* A suspended ray: its pool entries at `off` are its passed-over
+ * candidates (depth bits 8-10), then its DFS stack (bits 0-7); bit 11: its
+ * pixel already holds a hit found past those candidates. */
 struct SuspRec {
     unsigned int ray;
     unsigned int depth;
@@ -103,6 +107,7 @@ struct DevCtl {
     unsigned long long* pool_out; unsigned long long* pool_used; unsigned long long pool_cap;
     unsigned long long* req; unsigned int* n_req; unsigned int req_cap;
     int lookahead;                              /* bricks a suspended ray may request ahead */
+    int skip;                                   /* absent-brick candidates a ray may pass over */
     unsigned int* touched; int touch_shift;     /* optional bitmask of coarse nodes used (trace log) */
     unsigned long long touch_base;
 };
