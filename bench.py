@@ -760,6 +760,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     L = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch, predictor=P, warm=args.warm)
     if paging and P is not None:
         L.thr = paging["best"]["hint_threshold"]
+    skip_used = wl.r.tuning()["skip"]
     ms, per, launches, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index),
                                           cfg["l2flush"])
     tot_ms = sum(ms)
@@ -830,9 +831,9 @@ def run_ours(args, cfg, rank, world, torch, dist):
     W, H = cfg["W"], cfg["H"]
     if "views" in cfg:
         conf = {"views_per_launch": cfg["views"]["n"], "resolutions": [list(r) for r in cfg["views"]["res"]],
-                "rays_per_step": round(rays_rank / args.steps)}
+                "rays_per_step": round(rays_rank / args.steps), "skip": skip_used}
     else:
-        conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": wl.r.tuning()["skip"]}
+        conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": skip_used}
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
