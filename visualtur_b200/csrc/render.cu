@@ -437,10 +437,10 @@ __device__ __forceinline__ int candidate(const TraceArgs& A, Ray& R, unsigned lo
  * replaces it, and if none does it stands.  So a ray whose candidates lie
  * in several absent bricks asks for all of them in one pass instead of one
  * per pass, and the image is the one of the in-order traversal. */
-template <int VTYPE, bool SLAB, int U>
+template <int VTYPE, bool SLAB, int U, bool SKIP>
 __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, int budget) {
     const int Lo = A.oct.Lo;
-    if (SLAB) {
+    if (SKIP) {
         while (R.resumeSkips) {
             if (R.nskip == 0) {
                 R.resumeSkips = false;
@@ -455,11 +455,11 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
             if (c == CAND_HIT) { R.nskip = 0; R.resumeSkips = false; return RAY_DONE; }
         }
     }
-    const int K = (SLAB && !A.ctl.touched) ? A.ctl.skip : 0;
+    const int K = SKIP ? A.ctl.skip : 0;
     for (;;) {
         unsigned long long ent;
         for (;;) {
-            if (R.top < 0) return (SLAB && R.nskip > 0) ? RAY_SUSPENDED : RAY_DONE;   /* exhausted: background */
+            if (R.top < 0) return (SKIP && R.nskip > 0) ? RAY_SUSPENDED : RAY_DONE;   /* exhausted: background */
             ent = st.e[R.top];
             if (e_level(ent) == Lo) break;
             if (budget-- == 0) return RAY_RUNNING;
@@ -470,12 +470,12 @@ __device__ int run_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt, i
         if (budget-- == 0) return RAY_RUNNING;
         const int c = candidate<VTYPE, SLAB, U>(A, R, ent, cnt);
         if (c == CAND_MISSING) {
-            if (R.nskip < K) { st.sk[R.nskip++] = ent; R.top--; continue; }
+            if (SKIP && R.nskip < K) { st.sk[R.nskip++] = ent; R.top--; continue; }
             return RAY_SUSPENDED;   /* the candidate stays on the stack */
         }
         R.top--;
         if (c == CAND_HIT) {
-            if (!SLAB || R.nskip == 0) return RAY_DONE;
+            if (!SKIP || R.nskip == 0) return RAY_DONE;
             R.top = -1;             /* later candidates cannot matter */
             R.tent = true;
             return RAY_TENTATIVE;
@@ -522,7 +522,7 @@ __device__ __forceinline__ bool decode_ray(const DevView* sv, int nv, int tw, in
 /* Sets up work item w (pass 0: padded ray index; later passes: suspended
  * record).  Returns RAY_RUNNING when the ray has traversal to do, RAY_DONE
  * when it is background already (root miss), -1 for tile padding. */
-template <int VTYPE>
+template <int VTYPE, bool SKIP>
 __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, Ray& R, Stk& st,
                           unsigned int* cnt) {
     unsigned int depth = 0;
@@ -544,12 +544,15 @@ __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, 
     R.lastSlot = -1;
     R.nskip = 0; R.tent = false; R.resumeSkips = false;
     if (resume && depth > 0) {
-        const int nsk = (int)((depth >> 8) & 7u);
+        int nsk = 0;
+        if (SKIP) {
+            nsk = (int)((depth >> 8) & 7u);
+            R.nskip = nsk;
+            R.tent = (depth >> 11) & 1u;
+            R.resumeSkips = nsk > 0 || R.tent;
+            for (int e = 0; e < nsk; e++) st.sk[e] = A.ctl.pool_in[off + e];
+        }
         R.top = (int)(depth & 255u) - 1;
-        R.nskip = nsk;
-        R.tent = (depth >> 11) & 1u;
-        R.resumeSkips = nsk > 0 || R.tent;
-        for (int e = 0; e < nsk; e++) st.sk[e] = A.ctl.pool_in[off + e];
         for (int e = 0; e <= R.top; e++) st.e[e] = A.ctl.pool_in[off + nsk + e];
         return RAY_RUNNING;
     }
@@ -581,19 +584,19 @@ __device__ __forceinline__ void write_ray(const TraceArgs& A, const DevView* sv,
     }
 }
 
-template <int VTYPE, bool SLAB>
+template <int VTYPE, bool SLAB, bool SKIP>
 __device__ __forceinline__ void suspend_ray(const TraceArgs& A, Ray& R, Stk& st, unsigned int* cnt) {
     cnt[VT_C_SUSPENDED]++;
     unsigned int q = atomicAdd(A.ctl.n_out, 1u);
     if (q >= A.ctl.out_cap) { atomicOr(A.ctl.err, VT_KERR_SUSPEND_FULL); return; }
-    const unsigned int depth = (unsigned int)(R.top + 1), nsk = (unsigned int)R.nskip;
+    const unsigned int depth = (unsigned int)(R.top + 1), nsk = SKIP ? (unsigned int)R.nskip : 0u;
     unsigned long long off = atomicAdd(A.ctl.pool_used, (unsigned long long)(depth + nsk));
     SuspRec rec;
     rec.ray = R.g;
     if (off + depth + nsk <= A.ctl.pool_cap) {
         for (unsigned int e = 0; e < nsk; e++) A.ctl.pool_out[off + e] = st.sk[e];
         for (unsigned int e = 0; e < depth; e++) A.ctl.pool_out[off + nsk + e] = st.e[e];
-        rec.depth = depth | (nsk << 8) | ((R.tent ? 1u : 0u) << 11); rec.off = off;
+        rec.depth = depth | (nsk << 8) | ((SKIP && R.tent ? 1u : 0u) << 11); rec.off = off;
     } else {
         rec.depth = 0; rec.off = 0;   /* pool full: the ray restarts from the root (same result) */
     }
@@ -622,7 +625,7 @@ __device__ __forceinline__ void flush_counters(const TraceArgs& A, unsigned int*
  * Eight 128-thread CTAs per SM (64 registers a thread): the traversal is
  * latency-bound, and the extra resident warps hide more of it than the
  * few spilled registers cost. */
-template <int VTYPE, bool SLAB, bool PERSIST, int U>
+template <int VTYPE, bool SLAB, bool PERSIST, int U, bool SKIP>
 __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
     __shared__ DevView sv[VT_MAX_VIEWS];
     for (int k = threadIdx.x; k < A.views.n; k += blockDim.x) sv[k] = A.views.v[k];
@@ -636,11 +639,13 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
     if (!PERSIST) {
         unsigned int w = blockIdx.x * blockDim.x + threadIdx.x;
         if (w < nItems) {
-            int s = start_ray<VTYPE>(A, sv, w, R, st, cnt);
-            if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB, U>(A, R, st, cnt, -1);
-            if (s == RAY_DONE) write_ray(A, sv, R, cnt, !R.tent);
-            else if (s == RAY_TENTATIVE) { write_ray(A, sv, R, cnt); suspend_ray<VTYPE, SLAB>(A, R, st, cnt); }
-            else if (s == RAY_SUSPENDED) suspend_ray<VTYPE, SLAB>(A, R, st, cnt);
+            int s = start_ray<VTYPE, SKIP>(A, sv, w, R, st, cnt);
+            if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB, U, SKIP>(A, R, st, cnt, -1);
+            if (s == RAY_DONE) write_ray(A, sv, R, cnt, !(SKIP && R.tent));
+            else if (SKIP && s == RAY_TENTATIVE) {
+                write_ray(A, sv, R, cnt);
+                suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt);
+            } else if (s == RAY_SUSPENDED) suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt);
         }
     } else {
         const unsigned int lane = threadIdx.x & 31;
@@ -656,21 +661,21 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
                 if (!has) {
                     unsigned int w = base + __popc(need & ((1u << lane) - 1u));
                     if (w < nItems) {
-                        int s = start_ray<VTYPE>(A, sv, w, R, st, cnt);
+                        int s = start_ray<VTYPE, SKIP>(A, sv, w, R, st, cnt);
                         has = s == RAY_RUNNING;
                         if (s == RAY_DONE) write_ray(A, sv, R, cnt);
                     }
                 }
             }
             if (has) {
-                int s = run_ray<VTYPE, SLAB, U>(A, R, st, cnt, A.pops);
-                if (s == RAY_DONE) { write_ray(A, sv, R, cnt, !R.tent); has = false; }
-                else if (s == RAY_TENTATIVE) {
+                int s = run_ray<VTYPE, SLAB, U, SKIP>(A, R, st, cnt, A.pops);
+                if (s == RAY_DONE) { write_ray(A, sv, R, cnt, !(SKIP && R.tent)); has = false; }
+                else if (SKIP && s == RAY_TENTATIVE) {
                     write_ray(A, sv, R, cnt);
-                    suspend_ray<VTYPE, SLAB>(A, R, st, cnt);
+                    suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt);
                     has = false;
-                } else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB>(A, R, st, cnt); has = false; }
-                else if (s == RAY_DONE_WRITTEN) has = false;
+                } else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt); has = false; }
+                else if (SKIP && s == RAY_DONE_WRITTEN) has = false;
             }
         }
     }
@@ -801,14 +806,18 @@ cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, bool persistent, 
     } else {
         blocks = (items + threads - 1) / threads;
     }
-#define VT_LAUNCH_U(V, S, P)                                            \
-    switch (a.unroll) {                                                 \
-        case 2: k_trace<V, S, P, 2><<<blocks, threads, 0, s>>>(a); break; \
-        case 4: k_trace<V, S, P, 4><<<blocks, threads, 0, s>>>(a); break; \
-        case 8: k_trace<V, S, P, 8><<<blocks, threads, 0, s>>>(a); break; \
-        default: k_trace<V, S, P, 1><<<blocks, threads, 0, s>>>(a); break; \
+    /* setting absent bricks aside is compiled into its own kernels, so the
+     * in-order traversal keeps its registers; it needs bricks (slab mode)
+     * and is off while a trace is logged */
+    const bool skip = slabMode && a.ctl.skip > 0 && !a.ctl.touched;
+#define VT_LAUNCH_U(V, S, P, K)                                            \
+    switch (a.unroll) {                                                    \
+        case 2: k_trace<V, S, P, 2, K><<<blocks, threads, 0, s>>>(a); break; \
+        case 4: k_trace<V, S, P, 4, K><<<blocks, threads, 0, s>>>(a); break; \
+        case 8: k_trace<V, S, P, 8, K><<<blocks, threads, 0, s>>>(a); break; \
+        default: k_trace<V, S, P, 1, K><<<blocks, threads, 0, s>>>(a); break; \
     }
-#define VT_LAUNCH(V, S, P) VT_LAUNCH_U(V, S, P)
+#define VT_LAUNCH(V, S, P) { if (S && skip) VT_LAUNCH_U(V, S, P, S) else VT_LAUNCH_U(V, S, P, false) }
     if (a.br.vtype == 0) {
         if (slabMode) { if (persistent) VT_LAUNCH(0, true, true) else VT_LAUNCH(0, true, false) }
         else { if (persistent) VT_LAUNCH(0, false, true) else VT_LAUNCH(0, false, false) }
