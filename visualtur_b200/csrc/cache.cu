@@ -324,10 +324,13 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
     std::sort(spec.begin(), spec.end());
     int64_t disk = 0, loaded = 0;
     vt_status st;
-    /* chunk size: large services in chunks of 8 192 bricks; small ones (a
+    /* chunk size: large services in chunks of 4 096 bricks (the first
+     * chunk's reads and the last one's transfer are not overlapped: 8 192
+     * left 6 ms of transfer waiting at the end of the c2 cold start, 4 096
+     * leaves 3.5); small ones (a
      * steady-state pass) still in four, so the reads of one overlap the
      * transfer of the one before */
-    const size_t kChunk = std::min<size_t>(8192, std::max<size_t>(64, ((size_t)nReq + 3) / 4));
+    const size_t kChunk = std::min<size_t>(4096, std::max<size_t>(64, ((size_t)nReq + 3) / 4));
     /* host slots touched in this service stay put until it returns: fills of
      * earlier chunks may still be reading them */
     const uint64_t svcStart = tick_ + 1;
