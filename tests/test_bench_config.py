@@ -1,0 +1,34 @@
+"""The bench's workload table and tuner candidates, checked on the CPU:
+the plain renderer stays the reference's scheme, and every paging
+candidate is a setting the library accepts."""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_plain_mode_is_the_reference_scheme():
+    o = bench.MODES["plain"]["opts"]
+    assert o["lookahead"] == 0 and o.get("skip", 0) == 0 and o["persistent"] == 0 and o["use_graph"] == 0
+    assert bench.MODES["plain"]["batch"] == 1 and not bench.MODES["plain"]["learned"]
+
+
+def test_paging_candidates_are_valid_settings():
+    seen = set()
+    for b, la, sk in bench.PAGING_CANDIDATES:
+        assert b >= 1 and 0 <= la <= 64 and 0 <= sk <= 4
+        assert (b, la, sk) not in seen
+        seen.add((b, la, sk))
+    assert any(sk == 0 for _, _, sk in bench.PAGING_CANDIDATES)   # the in-order traversal is always a candidate
+    for t in bench.HINT_THRESHOLDS:
+        assert t is None or 0.0 < t < 1.0
+
+
+def test_every_workload_names_its_shape():
+    for name, c in bench.CONFIGS.items():
+        assert c["workload"] and c["W"] > 0 and c["H"] > 0, name
+        assert c["inc"] >= 3 and c["levelC"] <= c["levelO"], name
+        assert c["resident"] or c["dev_bytes"] > 0, name

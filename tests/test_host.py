@@ -104,3 +104,40 @@ def test_raw_volume_roundtrip(workdir):
     assert fm.vtype == vt.VT_U8 and np.array_equal(fm.readHDF5(), u8)
     assert np.array_equal(fm.readHDF5_Voxel_Array((-1, 0, 2), (3, 5, 8)),
                           orc.read_voxels(u8.astype(np.float32), (-1, 0, 2), (3, 5, 8)))
+
+
+LAYOUT_STRUCTS = ("vt_camera", "vt_params", "vt_options", "vt_stats", "vt_h5_info", "vt_tuning", "vt_view")
+
+
+def test_ctypes_mirrors_match_the_header(workdir):
+    """Every ctypes mirror of a vt.h struct has the C compiler's size and
+    field offsets (a field added on one side only shifts the rest)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "vt.h"', "int main(void) {"]
+    for s in LAYOUT_STRUCTS:
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (s, s))
+        for name, _ in getattr(vt, s)._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (s, name, s, name))
+    lines.append("return 0; }")
+    src = os.path.join(workdir, "layout.c")
+    exe = os.path.join(workdir, "layout")
+    open(src, "w").write("\n".join(lines) + "\n")
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(F.ROOT, "include"), src, "-o", exe], check=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for s in LAYOUT_STRUCTS:
+        T = getattr(vt, s)
+        assert got[(s, "size")] == ctypes.sizeof(T), s
+        for name, _ in T._fields_:
+            assert got[(s, name)] == getattr(T, name).offset, (s, name)
+
+
+def test_default_options_keep_the_reference_order():
+    """Defaults: demand paging without lookahead or set-aside candidates
+    (the reference's in-order scheme), single linear refinement."""
+    o = vt.default_options()
+    assert o.lookahead == 0 and o.skip == 0 and o.refine == 0 and o.resident == 0
