@@ -643,6 +643,7 @@ def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=Fa
 PAGING_CANDIDATES = ((8, 2, 0), (4, 2, 0), (2, 2, 0), (1, 2, 0), (1, 0, 0),
                      (4, 2, 4), (2, 2, 4), (4, 0, 4), (2, 0, 4), (1, 0, 4))
 HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
+VIEWS_PAGING = ((2, 0), (0, 0), (2, 2), (0, 2))                 # batched views: (lookahead, skip)
 
 
 def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
@@ -718,6 +719,28 @@ def autotune(args, wl, cfg, torch, dev, stream, frame0, batch):
     best, table = at.tune_schedule(torch, wl.r, lambda rr, i, s_: Lt.launch(items), frames=frames, stream=stream)
     if bricks:
         best = dict(best, brick=wl.brick)
+    if "views" in cfg and not cfg["resident"] and args.skip is None:
+        # lookahead requests and set-aside candidates, from a cold cache on
+        # two batches of another stretch of the workload
+        stretch = [Lt.cams(frame0 + 50 + k, batch) for k in range(2)]
+        prow = []
+        for la, sk in VIEWS_PAGING:
+            wl.r.set_tuning(lookahead=la, skip=sk)
+            wl.r.drop_cache()
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                torch.cuda.synchronize()
+                a.record(stream)
+                for it in stretch:
+                    Lt.launch(it)
+                e.record(stream)
+                torch.cuda.synchronize()
+            prow.append({"lookahead": la, "skip": sk, "ms": round(a.elapsed_time(e), 2)})
+            log("autotune: lookahead %d, skip %d -> %.1f ms for 2 batches" % (la, sk, prow[-1]["ms"]))
+        bp = min(prow, key=lambda x: x["ms"])
+        wl.r.set_tuning(lookahead=bp["lookahead"], skip=bp["skip"])
+        best = dict(best, lookahead=bp["lookahead"], skip=bp["skip"])
+        table = table + prow
     log("autotune: best %s" % best)
     if not cfg["resident"]:
         wl.r.drop_cache()

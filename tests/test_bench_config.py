@@ -32,3 +32,9 @@ def test_every_workload_names_its_shape():
         assert c["workload"] and c["W"] > 0 and c["H"] > 0, name
         assert c["inc"] >= 3 and c["levelC"] <= c["levelO"], name
         assert c["resident"] or c["dev_bytes"] > 0, name
+
+
+def test_views_paging_candidates_are_valid_settings():
+    assert (2, 0) in bench.VIEWS_PAGING          # the mode's own setting stays a candidate
+    for la, sk in bench.VIEWS_PAGING:
+        assert 0 <= la <= 64 and 0 <= sk <= 4
