@@ -17,7 +17,7 @@ A step is one rendered frame of the workload (one batch of views for c3):
       drawn from {256^2, 512^2, 1024^2, 1920x1080, 2048^2}; the autotuner
       also picks the brick edge {8, 16, 32}.
   c4: the c2 volume on a held-out 300-frame spline (the learned-prefetch
-      judgement: hit rate, stall per frame, same pixels as plain).
+      evaluation: hit rate, stall per frame, same pixels as plain).
   c5: 4096^3 uint8 fractal, 32^3 bricks, 16 GB cache, 600-frame spline.
   c2s / c3s / c5s: c2 / c3 / c5 at half the edge (profiling and quick checks).
 value = rays of all ranks / device time (CUDA events, max over ranks).
@@ -63,7 +63,7 @@ CONFIGS = {
                dist=50.0, resident=0, l2flush=False, orbit=(3000.0, 1.2), dev_bytes=4 << 30,
                host_bytes=16 << 30, blobs=(256, 20.0, 120.0, 0.5, 1.5, 0.05)),
     # 64 seeded views per launch, mixed resolutions, on the c2 volume
-    # the learned-prefetch judgement: the c2 volume on a held-out spline
+    # the learned-prefetch evaluation: the c2 volume on a held-out spline
     "c4": dict(workload="2048^3 f32 blobs+noise (the c2 volume), held-out 300-frame Catmull-Rom spline through 12 "
                         "seeded control points at r 2500-3500 looking into the inner half, 1920x1080, 4 GB device "
                         "cache, 16 GB pinned host tier, prefetch network trained on 20 000 poses of other "
