@@ -799,7 +799,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     t_max = max_over_ranks(dist, torch, tot_ms, dev)
     value = replica_value(rays_rank, world, t_max)
     # end to end through the public API: poses in, RGB8 images back in pinned host memory
-    e2e_steps = max(batch, 2 * batch if batch > 1 else (4 if "views" in cfg else 30))
+    e2e_steps = max(batch, 8 * batch if batch > 1 else (4 if "views" in cfg else 30))
     maxb = max(b.numel() for b, _ in L.outputs(L.cams(frame0, batch)))
     host8 = [torch.empty(maxb, dtype=torch.uint8, pin_memory=True) for _ in range(64)]
     torch.cuda.synchronize()
