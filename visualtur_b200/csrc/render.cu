@@ -8,7 +8,10 @@
  * walks its DFS, marches every candidate node whose brick is resident, and
  * either finishes or suspends with its stack saved when a brick is absent.
  * The result equals the reference's iterate-until-PAINTED loop: candidates
- * are marched in the same DFS order and the first hit is shaded.
+ * are marched in the same DFS order and the first hit is shaded.  The
+ * instantiations with SKIP = true let a ray set absent-brick candidates
+ * aside and march later ones in the same pass (see run_ray); the first hit
+ * in DFS order still decides the pixel.
  *
  * Octree: a flattened node array with 8-bit child masks holding the result
  * of the reference's range search (computed once per octree load), so a
