@@ -186,58 +186,102 @@ def huge_page_array(shape, dtype):
     return m, np.frombuffer(m, dtype).reshape(shape)
 
 
-def orbit_camera(vt, cfg, frame):
+# Poses of the workloads, as plain numbers: both arms turn them into their
+# own camera (libvt's vt_camera for the product, the oracle's camera for the
+# reference arm, which must not load libvt.so).  A pose is (W, H, position,
+# look, up, right) in float32; h and w come from the camera's own init.
+def _unit(v):
+    v = np.asarray(v, np.float32)
+    return (v / np.sqrt(np.float32((v * v).sum()))).astype(np.float32)
+
+
+def look_at_pose(W, H, pos, target, up=(0.0, 1.0, 0.0)):
+    """Pose at `pos` looking at `target` (right = cross(look, up), the
+    reference's basis convention; up re-orthogonalised)."""
+    pos = np.asarray(pos, np.float32)
+    look = _unit(np.asarray(target, np.float32) - pos)
+    upv = np.asarray(up, np.float32)
+    right = np.cross(look, upv).astype(np.float32)
+    if np.linalg.norm(right) < 1e-6:
+        upv = np.array([1, 0, 0], np.float32)
+        right = np.cross(look, upv).astype(np.float32)
+    upv = np.cross(right, look).astype(np.float32)
+    upv /= np.float32(np.linalg.norm(upv))
+    right = np.cross(look, upv).astype(np.float32)
+    return (W, H, pos, look, upv, right)
+
+
+def orbit_pose(cfg, frame):
     """Pose on the orbit: position c + r (sin a, 0, cos a), looking at c, up +y,
-    right = cross(look, up) (the reference's basis convention)."""
+    right = cross(look, up)."""
     r, step = cfg["orbit"]
     c = (cfg["n"] - 1) / 2.0
     a = math.radians(step * frame)
-    cam = vt.Camera(cfg["H"], cfg["W"], cfg["dist"], cfg["fov"], cfg["fov"]).c
     pos = np.array([c + r * math.sin(a), c, c + r * math.cos(a)], np.float32)
-    look = (np.array([c, c, c], np.float32) - pos)
-    look = (look / np.sqrt(np.float32((look * look).sum()))).astype(np.float32)
+    look = _unit(np.array([c, c, c], np.float32) - pos)
     up = np.array([0, 1, 0], np.float32)
-    right = np.cross(look, up).astype(np.float32)
-    for i in range(3):
-        cam.look[i], cam.up[i], cam.right[i], cam.position[i] = look[i], up[i], right[i], pos[i]
-    return cam
+    return (cfg["W"], cfg["H"], pos, look, up, np.cross(look, up).astype(np.float32))
 
 
-def static_camera(vt, cfg):
-    cam = vt.Camera(cfg["H"], cfg["W"], cfg["dist"], cfg["fov"], cfg["fov"])
-    cam.Move(cfg["cam_pos"])
-    return cam.c
+def static_pose(cfg):
+    """The reference camera's initial basis (look -z, up +y), moved to cam_pos."""
+    look, up = np.array([0, 0, -1], np.float32), np.array([0, 1, 0], np.float32)
+    return (cfg["W"], cfg["H"], np.asarray(cfg["cam_pos"], np.float32), look, up, np.cross(look, up).astype(np.float32))
+
+
+def catmull_rom(points, frames):
+    """Uniform Catmull-Rom spline through `points` (closed), `frames` samples."""
+    P = np.asarray(points, np.float64)
+    k = len(P)
+    out = []
+    for f in range(frames):
+        u = f * k / frames
+        i = int(u)
+        t = u - i
+        p0, p1, p2, p3 = P[(i - 1) % k], P[i % k], P[(i + 1) % k], P[(i + 2) % k]
+        out.append(0.5 * ((2 * p1) + (-p0 + p2) * t + (2 * p0 - 5 * p1 + 4 * p2 - p3) * t * t +
+                          (-p0 + 3 * p1 - 3 * p2 + p3) * t * t * t))
+    return np.array(out)
+
+
+def flythrough(rng, n, frames, r_lo, r_hi, ctrl):
+    """Positions on a spline through `ctrl` random points at radius
+    [r_lo, r_hi] around the volume centre, looking at points of a spline
+    through random targets in the volume's inner half."""
+    c = (n - 1) / 2.0
+    v = rng.standard_normal((ctrl, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    pos = catmull_rom(c + v * rng.uniform(r_lo, r_hi, (ctrl, 1)), frames)
+    tgt = catmull_rom(c + rng.uniform(-n / 4, n / 4, (ctrl, 3)), frames)
+    return pos, tgt
 
 
 _PATHS = {}
 
 
-def path_camera(cfg, frame):
-    """Pose `frame` of a seeded Catmull-Rom fly-through: positions through
-    cfg["path"]["ctrl"] control points on a shell around the volume, looking
-    at a spline through targets in the inner half (frames wrap around)."""
-    from visualtur_b200 import prefetch as pf
+def path_pose(cfg, frame):
+    """Pose `frame` of the workload's seeded Catmull-Rom fly-through (frames
+    wrap around)."""
     spec, n = cfg["path"], cfg["n"]
     key = (cfg["seed"], n, spec["frames"])
     if key not in _PATHS:
-        _PATHS[key] = pf.random_flythrough(np.random.default_rng([cfg["seed"], 5]), n, spec["frames"],
-                                           spec["r"][0], spec["r"][1], ctrl=spec["ctrl"])
+        _PATHS[key] = flythrough(np.random.default_rng([cfg["seed"], 5]), n, spec["frames"], spec["r"][0],
+                                 spec["r"][1], spec["ctrl"])
     pos, tgt = _PATHS[key]
     f = frame % spec["frames"]
-    return pf.look_at(cfg["W"], cfg["H"], cfg["dist"], cfg["fov"], pos[f], tgt[f])
+    return look_at_pose(cfg["W"], cfg["H"], pos[f], tgt[f])
 
 
-def frame_camera(vt, cfg, frame):
+def frame_pose(cfg, frame):
     if cfg.get("path"):
-        return path_camera(cfg, frame)
-    return orbit_camera(vt, cfg, frame) if cfg["orbit"] else static_camera(vt, cfg)
+        return path_pose(cfg, frame)
+    return orbit_pose(cfg, frame) if cfg["orbit"] else static_pose(cfg)
 
 
-def step_views(cfg, step):
+def step_poses(cfg, step):
     """The seeded views of one batched step: positions uniform on a sphere
     shell around the volume centre, targets uniform in the inner half,
     resolution drawn uniformly from the config's list."""
-    from visualtur_b200 import prefetch as pf
     spec, n = cfg["views"], cfg["n"]
     rng = np.random.default_rng([cfg["seed"], 3, step])
     c = (n - 1) / 2.0
@@ -247,8 +291,35 @@ def step_views(cfg, step):
         pos = c + v / np.linalg.norm(v) * rng.uniform(*spec["r"])
         tgt = c + rng.uniform(-n / 4.0, n / 4.0, 3)
         W, H = spec["res"][int(rng.integers(len(spec["res"])))]
-        out.append(pf.look_at(W, H, cfg["dist"], cfg["fov"], pos, tgt))
+        out.append(look_at_pose(W, H, pos, tgt))
     return out
+
+
+def vt_cam(vt, cfg, pose):
+    """libvt camera (vt_camera) of a pose."""
+    W, H, pos, look, up, right = pose
+    cam = vt.Camera(H, W, cfg["dist"], cfg["fov"], cfg["fov"]).c
+    for i in range(3):
+        cam.look[i], cam.up[i], cam.right[i], cam.position[i] = look[i], up[i], right[i], pos[i]
+    return cam
+
+
+def oracle_cam(orc, cfg, pose):
+    """The oracle's camera of a pose."""
+    W, H, pos, look, up, right = pose
+    cam = orc.Camera(H, W, cfg["dist"], cfg["fov"], cfg["fov"])
+    for name, v in (("look", look), ("up", up), ("right", right), ("position", pos)):
+        setattr(cam.c, name, orc.orc_f3(float(v[0]), float(v[1]), float(v[2])))
+    return cam
+
+
+def frame_camera(vt, cfg, frame):
+    return vt_cam(vt, cfg, frame_pose(cfg, frame))
+
+
+def step_views(cfg, step):
+    import visualtur_b200 as vt
+    return [vt_cam(vt, cfg, p) for p in step_poses(cfg, step)]
 
 
 class Workload:
@@ -370,6 +441,19 @@ def roofline(stats_frames, trace_ms, pixels, traffic_per_ray=None, esize=4):
             "kernel": "k_trace"}
 
 
+def workload_config(cfg, name, world):
+    """The `config` of both arms' lines: what the workload is, nothing the
+    renderer chose (the product's tuned settings go under "renderer")."""
+    conf = {"workload": cfg["workload"], "name": name,
+            "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+    if "views" in cfg:
+        conf.update(views_per_launch=cfg["views"]["n"], resolutions=[list(r) for r in cfg["views"]["res"]])
+    else:
+        conf.update(W=cfg["W"], H=cfg["H"])
+    return conf
+
+
 def hint_use(P, conf):
     """How the timed run uses the learned prefetcher: a network is trained
     for every out-of-core workload, and the paging tuner decides whether its
@@ -382,24 +466,20 @@ def hint_use(P, conf):
     return "hints on (threshold %g)" % thr
 
 
-def sample_camera(cfg, step):
-    """The camera the CPU baseline renders for `step`: the frame's camera,
-    or the first view of a batched step."""
-    import visualtur_b200 as vt
-    return step_views(cfg, step)[0] if "views" in cfg else frame_camera(vt, cfg, step)
+def sample_pose(cfg, step):
+    """The pose the CPU baseline renders for `step`: the frame's pose, or the
+    first view of a batched step."""
+    return step_poses(cfg, step)[0] if "views" in cfg else frame_pose(cfg, step)
 
 
-def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0, octree=None, per_ray=None):
+def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0, octree=None, per_ray=None, keep=False):
     """Oracle (CPU restatement of the reference algorithm) on a bounded ray
     sample of step `step`'s camera; returns rays/s (with "per_ray_s", the
     probe's seconds per ray, to size later samples without probing)."""
     from oracle import oracle as orc
     o = octree if octree is not None else orc.Octree(octree_path)
-    c = sample_camera(cfg, step)
-    cam = orc.Camera(c.H, c.W, cfg["dist"], cfg["fov"], cfg["fov"])
-    for f in ("look", "up", "right", "position"):
-        v = getattr(c, f)
-        setattr(cam.c, f, orc.orc_f3(v[0], v[1], v[2]))
+    cam = oracle_cam(orc, cfg, sample_pose(cfg, step))
+    c = cam.c
     n = c.W * c.H
     stride = 1
     # probe a sparse sample, then size the sample to the time budget
@@ -413,16 +493,29 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0, octree=None
     reps = 0
     rays = 0
     while True:
-        orc.render(o, wl.volume, cam, cfg["levelO"], cfg["levelC"], cfg["inc"], nthreads=nthreads, ray_stride=stride)
+        out = orc.render(o, wl.volume, cam, cfg["levelO"], cfg["levelC"], cfg["inc"], nthreads=nthreads,
+                         ray_stride=stride)
         rays += (n + stride - 1) // stride
         reps += 1
         if time.perf_counter() - t0 > budget_s * 0.5 or stride > 1:
             break
     el = time.perf_counter() - t0
     threads = nthreads or os.cpu_count()
-    return {"value": round(rays / el, 1), "unit": "rays/s", "cores": threads, "kind": "port",
-            "sample": "%d x every %d-th ray of a %dx%d view of step %d (%d rays, %.1f s)" %
-                      (reps, stride, c.W, c.H, step, rays, el), "per_ray_s": el / max(rays, 1)}
+    res = {"value": round(rays / el, 1), "unit": "rays/s", "cores": threads, "kind": "port",
+           "sample": "%d x every %d-th ray of a %dx%d view of step %d (%d rays, %.1f s)" %
+                     (reps, stride, c.W, c.H, step, rays, el), "per_ray_s": el / max(rays, 1)}
+    if keep:
+        res["_oracle"] = (out, stride)
+    return res
+
+
+def oracle_mismatch(product_rgba, oracle):
+    """Rays of the oracle's sample whose product RGBA differs in any bit."""
+    out, stride = oracle
+    a = product_rgba[::stride].view(np.uint32)
+    b = out["rgba"][::stride].view(np.uint32)
+    return {"oracle_checked_rays": int(a.shape[0]), "oracle_mismatch_rays": int((a != b).any(axis=1).sum()),
+            "oracle_hits": int((out["node"][::stride] != 0).sum())}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -541,6 +634,58 @@ class ViewLauncher:
                 self.r.render_batch([v], stream=sp)
         else:
             self.r.render_batch(views, stream=sp)
+
+
+def run_e2e(L, launches, cfg, torch, dev, stream, dist, world):
+    """The timed steps again through the public API (vt_render /
+    vt_render_batch) from a cold cache, with each step's RGB8 images copied
+    to pinned host memory inside the step: host wall clock, max over ranks."""
+    r = L.r
+    maxb = max(b.numel() for b, _ in L.outputs(launches[0][2]))
+    host8 = [torch.empty(maxb, dtype=torch.uint8, pin_memory=True) for _ in range(64)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if cfg["l2flush"] else None
+    torch.cuda.synchronize()
+    if not cfg["resident"] and not L.warm:
+        r.drop_cache()
+        if L.P is not None:
+            L.P.reset_hints()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    rays = d2h = 0
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for f0, n, cams, nxt in launches:
+            if flush is not None:
+                flush.zero_()
+            L.launch(cams, nxt, f0)
+            for i, (b, nb) in enumerate(L.outputs(cams)):
+                host8[i][:nb].copy_(b[:nb], non_blocking=True)
+                d2h += nb
+            rays += L.rays(cams)
+            stream.synchronize()
+    wall_ms = max_over_ranks(dist, torch, (time.perf_counter() - t0) * 1e3, dev)
+    import ctypes
+    per_view = ctypes.sizeof(L.wl.vt.vt_camera)
+    steps = sum(n for _, n, _, _ in launches) if "views" not in cfg else len(launches)
+    views_per_step = cfg["views"]["n"] if "views" in cfg else 1
+    return {"value": round(rays * world / (wall_ms * 1e-3), 1), "unit": "rays/s",
+            "h2d_bytes_per_step": per_view * views_per_step, "d2h_bytes_per_step": int(d2h / steps),
+            "ms_per_step": round(wall_ms / steps, 4), "steps": steps,
+            "note": "the timed steps again from a cold cache: host wall clock around the public API "
+                    "(vt_render / vt_render_batch; camera poses in) plus the D2H copy of every RGB8 image "
+                    "into pinned host memory; brick transfers from the host tier are inside the render calls"}
+
+
+def product_frame_rgba(vtm, r, cam, torch, dev, stream):
+    """RGBA of one view rendered by renderer `r` (any resolution)."""
+    buf = torch.empty(cam.W * cam.H * 4, dtype=torch.float32, device=dev)
+    v = vtm.vt_view()
+    v.cam, v.dev_rgba, v.dev_rgb8 = cam, buf.data_ptr(), None
+    with torch.cuda.stream(stream):
+        r.render_batch([v], stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    return buf.cpu().numpy().reshape(-1, 4)
 
 
 def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, label="timed"):
@@ -798,32 +943,14 @@ def run_ours(args, cfg, rank, world, torch, dist):
     rays_rank = sum(L.rays(cams) for _, _, cams, _ in launches)
     t_max = max_over_ranks(dist, torch, tot_ms, dev)
     value = replica_value(rays_rank, world, t_max)
-    # end to end through the public API: poses in, RGB8 images back in pinned host memory
-    e2e_steps = max(batch, 8 * batch if batch > 1 else (4 if "views" in cfg else 30))
-    maxb = max(b.numel() for b, _ in L.outputs(L.cams(frame0, batch)))
-    host8 = [torch.empty(maxb, dtype=torch.uint8, pin_memory=True) for _ in range(64)]
-    torch.cuda.synchronize()
-    f = frame0 + args.warmup + args.steps
-    e2e_rays = d2h = h2d = 0
-    t0 = time.perf_counter()
-    with torch.cuda.stream(stream):
-        for k in range(0, e2e_steps, batch):
-            cams = L.cams(f + k, batch)
-            L.launch(cams, L.cams(f + k + batch, batch), f + k)
-            for i, (b, nb) in enumerate(L.outputs(cams)):
-                host8[i][:nb].copy_(b[:nb], non_blocking=True)
-                d2h += nb
-            e2e_rays += L.rays(cams)
-            stream.synchronize()
-    e2e_s = max_over_ranks(dist, torch, (time.perf_counter() - t0) * 1e3, dev) * 1e-3
-    import ctypes
-    per_view = ctypes.sizeof(wl.vt.vt_camera)
-    views_per_step = cfg["views"]["n"] if "views" in cfg else 1
-    e2e = {"value": round(e2e_rays / e2e_s * world, 1), "unit": "rays/s",
-           "h2d_bytes_per_step": per_view * views_per_step, "d2h_bytes_per_step": int(d2h / e2e_steps),
-           "ms_per_step": round(e2e_s * 1e3 / e2e_steps, 3), "steps": e2e_steps,
-           "note": "continues the workload after the timed steps; wall clock around the public API "
-                   "(vt_render / vt_render_batch) plus the D2H copy of every RGB8 image"}
+    # end to end through the public API, over the same steps as the timed
+    # region and from the same cold cache: poses in, every RGB8 image back
+    # in pinned host memory before the step ends (wall clock, max over ranks)
+    e2e = run_e2e(L, launches, cfg, torch, dev, stream, dist, world)
+    # one frame of the timed workload through the product renderer, for the
+    # oracle comparison of the CPU baseline's ray sample
+    product_sample = product_frame_rgba(wl.vt, wl.r, vt_cam(wl.vt, cfg, sample_pose(cfg, frame0 + args.warmup)),
+                                        torch, dev, stream)
     # the plain LRU renderer on the same steps, for comparison
     plain = None
     check = None
@@ -868,10 +995,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
         "ms_per_step": round(t_max / args.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8" if wl.esize == 1 else "f32",
         "data": "synthetic (seeded generators, device-generated)",
-        "config": dict(conf, workload=cfg["workload"], name=args.config, mode=args.mode,
-                       learned_prefetch=hint_use(P, conf), brick=wl.brick, **{
-                   "l2": "flushed (256 MB write) between frames" if cfg["l2flush"] else "inputs larger than L2",
-                   "parallelism": "replicas" if world > 1 else "single GPU"}),
+        "config": workload_config(cfg, args.config, world),
+        "renderer": dict(conf, mode=args.mode, learned_prefetch=hint_use(P, conf), brick=wl.brick),
         "roofline": roofline(ld, trace_tot, rays_rank, TRAFFIC_BYTES_PER_RAY.get(args.config), wl.esize),
         "e2e": e2e,
         "clocks": clk,
@@ -907,8 +1032,11 @@ def run_ours(args, cfg, rank, world, torch, dist):
         if tune["bricks"]:
             line["autotune"]["bricks"] = tune["bricks"]
     if not args.no_cpu_baseline:
-        cb = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, step=frame0 + args.warmup)
+        cb = cpu_baseline(cfg, wl, wl.octree_path, args.cpu_budget, step=frame0 + args.warmup, keep=True)
         cb.pop("per_ray_s")
+        # the product's pixels of the same rays against the oracle's
+        line["oracle_check"] = dict(oracle_mismatch(product_sample, cb.pop("_oracle")),
+                                    frame="step %d (the first timed step)" % (frame0 + args.warmup))
         one = cpu_baseline(cfg, wl, wl.octree_path, max(1.0, args.cpu_budget / 3), nthreads=1,
                            step=frame0 + args.warmup)
         cb["value_1thread"] = one["value"]
@@ -917,14 +1045,53 @@ def run_ours(args, cfg, rank, world, torch, dist):
     return line
 
 
+class RefWorkload:
+    """The reference arm's inputs, made without libvt: the volume by the
+    torch restatement of the seeded generators (oracle/volumes.py, equal to
+    libvt's device generator bit for bit), the octree by the oracle's CPU
+    builder (the reference's algorithm, byte-identical files)."""
+
+    def __init__(self, cfg, torch, dev, workdir):
+        from oracle import oracle as orc
+        from oracle import volumes as V
+        n = cfg["n"]
+        u8 = cfg["gen"] == "fractal"
+        t0 = time.time()
+        self._host_map, arr = huge_page_array((n, n, n), np.uint8 if u8 else np.float32)
+        host = torch.from_numpy(arr)
+        if cfg["gen"] == "sphere":
+            c = (n - 1) / 2.0
+            kind, prm = "sphere", (c, c, c, 0.25)
+        elif u8:
+            kind, prm = "fractal", cfg["spheres"]
+        else:
+            kind, prm = "blobs", cfg["blobs"]
+        V.generate(torch, kind, cfg["seed"], (n, n, n), prm, host, dev, slab=max(1, (256 << 20) // (n * n)))
+        if dev.type == "cuda":
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+        self.volume = arr
+        t1 = time.time()
+        self.octree_path = os.path.join(workdir, "vol_%s.oct" % cfg["gen"])
+        orc.build_octree(self.volume, cfg["iso"], self.octree_path)
+        t2 = time.time()
+        log("reference setup: generate %.1fs (torch), octree %.1fs (oracle builder, CPU)" % (t1 - t0, t2 - t1))
+
+
 def run_reference(args, cfg, rank, world, torch):
+    """The reference's path is CUDA code with no CPU implementation; this
+    arm times its CPU restatement -- the oracle port of the reference's
+    camera, octree traversal, brick addressing and march -- on all host
+    threads, a bounded ray sample of every step's camera."""
     if rank != 0:
         return None
-    dev = torch.device("cuda", 0)
+    # the generators run on the GPU where there is one (the bench's boxes),
+    # else on the CPU (exact for the sphere and fractal volumes)
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
     work = tempfile.mkdtemp(prefix="vtbench_ref_")
-    wl = Workload(cfg, torch, dev, work, need_renderer=False)
+    wl = RefWorkload(cfg, torch, dev, work)
     if "views" in cfg:
-        n = sum(c.W * c.H for c in step_views(cfg, args.warmup))
+        n = sum(p[0] * p[1] for p in step_poses(cfg, args.warmup))
     else:
         n = cfg["W"] * cfg["H"]
     # the whole run samples about --ref-total seconds of CPU rendering
@@ -947,11 +1114,12 @@ def run_reference(args, cfg, rank, world, torch):
         "value": rays_s, "unit": "rays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(n / rays_s * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8" if cfg["gen"] == "fractal" else "f32", "data": "synthetic (seeded generators)",
-        "config": {"workload": cfg["workload"], "name": args.config, "W": cfg["W"], "H": cfg["H"]},
+        "config": workload_config(cfg, args.config, world),
         "cpu_baseline": dict(vals[-1], value=rays_s),
         "e2e": {"value": rays_s, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference's path is CUDA-only; this arm times its CPU restatement (oracle port) "
-                "on all host threads over a bounded ray sample per step",
+        "note": "vs CPU port: the reference's path is CUDA-only, so this arm times the reference algorithm's CPU "
+                "restatement (oracle/vt_oracle.cpp) on all host threads over a bounded ray sample per step; "
+                "inputs made without libvt (torch restatement of the generators, oracle CPU octree builder)",
     }
     return line
 

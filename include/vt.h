@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define VT_API_VERSION 1
+#define VT_API_VERSION 2
 
 typedef enum {
     VT_OK = 0,
@@ -64,6 +64,18 @@ typedef struct vt_volume vt_volume;
 vt_status vt_volume_open(const char* path, const char* dataset, vt_volume** out);
 /* Wraps caller-owned host memory as a volume (no copy; must outlive it). */
 vt_status vt_volume_wrap(const void* data, int vtype, const int64_t dims[3], vt_volume** out);
+/* A volume read through a caller's function (no reference counterpart):
+ * read(user, s, e, out) fills out with the voxels [s,e) as vt_volume_read
+ * would (|e-s| per axis, x slowest, zeros outside the volume, the volume's
+ * voxel type) and returns 0, or returns non-zero when the read failed (a
+ * short read, a missing brick file).  Brick-cache misses call it from
+ * several host threads at once.  A failed read makes the render call
+ * return VT_ERR_IO -- where the reference exit(0)s on an HDF5 error
+ * (src/FileManager.cu:15-36) -- and leaves the renderer usable: the next
+ * frame requests the brick again.  Volumes of this kind serve the brick
+ * cache and vt_volume_read only (not resident renderers or the builder). */
+typedef int (*vt_read_fn)(void* user, const int s[3], const int e[3], void* out);
+vt_status vt_volume_from_reader(vt_read_fn read, void* user, int vtype, const int64_t dims[3], vt_volume** out);
 void      vt_volume_close(vt_volume* v);
 vt_status vt_volume_info(const vt_volume* v, int64_t dims[3], int* vtype);
 /* FileManager::readHDF5_Voxel_Array (src/FileManager.cu:86-167): reads
@@ -193,6 +205,13 @@ typedef struct {
                               pass; a hit found past them waits for them, so the image
                               is the in-order one.  0 = stop at the first absent brick,
                               as the reference.  Off while record_trace is on. */
+    /* Bounds of a pass's queues (0 = sized so they never fill).  Requests
+     * past max_requests wait for the next pass (the reference's per-pass
+     * admission cap, src/lruCache.cu:184-192); more than max_suspended rays
+     * waiting on bricks fail the frame with VT_ERR_STATE; a suspended ray
+     * whose stack does not fit the pool of pool_per_ray entries per ray
+     * restarts from the root next pass (same pixel). */
+    int max_suspended, max_requests, pool_per_ray;
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -291,6 +310,7 @@ typedef struct {
     double  ms_host_read_total;     /* cumulative host time reading bricks into the host tier */
     double  ms_fill_wait_total;     /* cumulative host time waiting for device fills to finish */
     double  ms_wait_last_frame;     /* host time of the last frame blocked on its passes' results */
+    int64_t requests_deferred;      /* brick requests past max_requests, retried a pass later */
 } vt_stats;
 vt_status vt_get_stats(vt_handle* h, vt_stats* s);
 /* Empties the brick cache (both tiers): the next frame starts cold.
@@ -330,7 +350,9 @@ vt_status vt_mlp_set_weights(vt_mlp* m, const float* host, int64_t n);
  * so batch * (h1 + h2) must be at most 262144 floats (e.g. batch 256 for
  * 512 + 512 hidden units); larger batches return VT_ERR_INVALID.  The first
  * call on each device looks the array's address up (cudaGetSymbolAddress):
- * make that first call before any stream capture.  All calls on a device
+ * make that first call before any stream capture.  After a cudaDeviceReset
+ * the next call looks it up again, so make that call outside a capture too.
+ * All calls on a device
  * share the array: calls that overlap on the GPU (other streams, threads)
  * race and must be serialised by the caller. */
 vt_status vt_mlp_forward_noalloc(vt_mlp* m, const float* dev_x, int batch, float* dev_p, void* stream);

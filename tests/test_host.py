@@ -20,7 +20,7 @@ def test_library_exports_every_declared_symbol():
     L = ctypes.CDLL(vt.LIB_PATH)
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert vt.lib().vt_api_version() == 1
+    assert vt.lib().vt_api_version() == 2
 
 
 OPS = [("mv", (31.5, 31.5, 181.5)), ("ry", 10.0), ("rx", -8.0), ("rz", 5.0), ("mf", 20.0), ("sr", 3.0),

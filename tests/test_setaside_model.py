@@ -25,8 +25,11 @@ def in_order(cands, resident_at):
     return None, passes
 
 
-def set_aside(cands, resident_at, K):
-    """the kernel's rule: returns (hit index or None, passes)"""
+def set_aside(cands, resident_at, K, evict=None, max_passes=1000):
+    """the kernel's rule: returns (hit index or None, passes).  evict(loaded,
+    requested, passes) -> bricks the service between passes drops again
+    (never those it loads for this pass's requests, as the cache never
+    evicts a slot stamped by the pass that follows)."""
     passes, loaded = 1, set()
     pos, aside, tent = 0, [], None
     resume = False
@@ -75,8 +78,11 @@ def set_aside(cands, resident_at, K):
                 if not aside:
                     return None, passes
                 suspended = True
+        if evict is not None:
+            loaded -= evict(loaded - requested, requested, passes)
         loaded |= requested
         passes += 1
+        assert passes <= max_passes, "no progress"
         resume = True
 
 
@@ -95,3 +101,29 @@ def test_set_aside_keeps_the_in_order_pixel_and_never_adds_passes():
             got, p1 = set_aside(cands, resident_at, K)
             assert got == want, (cands, warm, K)
             assert p1 <= p0, (cands, warm, K)
+
+
+def test_set_aside_keeps_the_in_order_pixel_when_bricks_are_evicted_between_passes():
+    """Bricks loaded for earlier passes may be evicted again before the
+    set-aside candidates are marched: the resumed candidate then finds its
+    brick absent, requests it and suspends (the kernel's CAND_MISSING ->
+    RAY_SUSPENDED in the resume loop).  The pixel is still the in-order
+    one; the pass count may grow."""
+    rng = random.Random(11)
+    for _ in range(4000):
+        n = rng.randint(0, 12)
+        nbricks = rng.randint(1, 6)
+        cands = [(rng.randrange(nbricks), rng.random() < 0.25) for _ in range(n)]
+        warm = {b for b in range(nbricks) if rng.random() < 0.3}
+        evict_p = rng.choice((0.2, 0.5, 0.9))
+        # warm bricks are resident only in the first pass: later passes see
+        # them only once loaded, and loaded bricks can be evicted
+        def resident_at(b, p, warm=warm):
+            return p == 1 and b in warm
+
+        def evict(old, requested, p, evict_p=evict_p, r=rng):
+            return {b for b in old if r.random() < evict_p}
+        want = next((i for i, (_, hit) in enumerate(cands) if hit), None)
+        for K in (1, 2, 4):
+            got, _ = set_aside(cands, resident_at, K, evict=evict)
+            assert got == want, (cands, warm, K, evict_p)

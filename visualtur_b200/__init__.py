@@ -23,6 +23,9 @@ VT_GEN_SPHERE, VT_GEN_BLOBS, VT_GEN_FRACTAL_U8 = 0, 1, 2
 CAM_MOVE, CAM_ROTX, CAM_ROTY, CAM_ROTZ, CAM_FORWARD, CAM_UPWARD, CAM_STRAFE = range(7)
 
 
+READ_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p)
+
+
 class VtError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__("vt status %d: %s" % (status, msg))
@@ -47,7 +50,7 @@ class vt_options(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("resident", "tile_w", "tile_h", "unroll", "lookahead", "max_passes",
                                          "host_threads", "record_trace", "trace_level", "record_hits",
                                          "persistent", "blocks_per_sm", "pops", "preload", "use_graph", "refine",
-                                         "skip")]
+                                         "skip", "max_suspended", "max_requests", "pool_per_ray")]
 
 
 class vt_stats(C.Structure):
@@ -58,7 +61,8 @@ class vt_stats(C.Structure):
         "bricks_hinted", "bricks_staged", "bricks_speculative")] + \
         [(n, C.c_double) for n in ("ms_last_frame", "ms_stall_last_frame", "bytes_h2d_last_frame",
                                    "ms_trace_last_frame", "ms_prefetch_last_frame", "ms_host_read_total",
-                                   "ms_fill_wait_total", "ms_wait_last_frame")]
+                                   "ms_fill_wait_total", "ms_wait_last_frame")] + \
+        [("requests_deferred", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -89,6 +93,7 @@ _PROTOS = {
     "vt_api_version": (C.c_int, []),
     "vt_volume_open": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_P)]),
     "vt_volume_wrap": (C.c_int, [_P, C.c_int, _I64_3, C.POINTER(_P)]),
+    "vt_volume_from_reader": (C.c_int, [_P, _P, C.c_int, _I64_3, C.POINTER(_P)]),
     "vt_volume_close": (None, [_P]),
     "vt_volume_info": (C.c_int, [_P, _I64_3, C.POINTER(C.c_int)]),
     "vt_volume_read": (C.c_int, [_P, C.c_int * 3, C.c_int * 3, _P]),
@@ -212,6 +217,29 @@ class FileManager:
         h = C.c_void_p()
         check(lib().vt_volume_wrap(a.ctypes.data, vt, _d3(a.shape), C.byref(h)))
         return cls(_handle=h, _keep=a)
+
+    @classmethod
+    def from_reader(cls, read, dims, vtype=VT_F32):
+        """A volume read through `read(s, e) -> array or None`: the voxels
+        [s, e) as readHDF5_Voxel_Array returns them (zeros outside the
+        volume), or None when the read fails (the render call then raises
+        VtError with VT_ERR_IO).  Called from libvt's host threads."""
+        dt = np.uint8 if vtype == VT_U8 else np.float32
+
+        def cb(user, s, e, out):
+            try:
+                box = read(tuple(s[i] for i in range(3)), tuple(e[i] for i in range(3)))
+                if box is None:
+                    return 1
+                b = np.ascontiguousarray(box, dt)
+                C.memmove(out, b.ctypes.data, b.nbytes)
+                return 0
+            except Exception:
+                return 1
+        fn = READ_FN(cb)
+        h = C.c_void_p()
+        check(lib().vt_volume_from_reader(C.cast(fn, C.c_void_p), None, vtype, _d3(dims), C.byref(h)))
+        return cls(_handle=h, _keep=fn)
 
     def readHDF5_Voxel_Array(self, s, e):
         out = np.empty([abs(int(e[i]) - int(s[i])) for i in range(3)], np.float32)

@@ -51,18 +51,22 @@ def build(force=False, verbose=False):
     common = host + ["-std=c++17", "-O3", "-I" + os.path.join(ROOT, "include"), "-Xcompiler", xc]
     cuflags = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "--fmad=false",
                "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
-    objs = []
+    jobs = []
     for f in CU:
         o = os.path.join(BUILD, f + ".o")
-        out = _run([nvcc, "-c", os.path.join(CSRC, f), "-o", o] + common + cuflags +
-                   (["-Xptxas", "-v"] if verbose else []))
-        if verbose:
-            sys.stderr.write(out)
-        objs.append(o)
+        jobs.append((o, [nvcc, "-c", os.path.join(CSRC, f), "-o", o] + common + cuflags +
+                     (["-Xptxas", "-v"] if verbose else [])))
     for f in CPP:
         o = os.path.join(BUILD, f + ".o")
-        _run([nvcc, "-x", "c++", "-c", os.path.join(CSRC, f), "-o", o] + common)
-        objs.append(o)
+        jobs.append((o, [nvcc, "-x", "c++", "-c", os.path.join(CSRC, f), "-o", o] + common))
+    # translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        outs = list(ex.map(lambda j: _run(j[1]), jobs))
+    if verbose:
+        for out in outs:
+            sys.stderr.write(out)
+    objs = [o for o, _ in jobs]
     tmp = LIB + ".tmp"
     _run([nvcc, "-shared", "-o", tmp] + objs + host +
          ["-Xcompiler", "-fopenmp", "-lcudart", "-lgomp", "-gencode", "arch=compute_100a,code=sm_100a"])

@@ -290,6 +290,7 @@ done:
 extern "C" vt_status vt_octree_build(const vt_volume* v, float iso, const char* out_path, void* stream) {
     vtrt::clear_error();
     if (!v || !out_path) return vtrt::fail(VT_ERR_INVALID, "vt_octree_build: null argument");
+    if (!v->data) return vtrt::fail(VT_ERR_UNSUPPORTED, "vt_octree_build: the volume is read through a function");
     size_t bytes = v->voxels() * v->esize();
     void* d = nullptr;
     cudaError_t e = cudaMalloc(&d, bytes);

@@ -48,6 +48,12 @@ __global__ void k_page_update(int* page, const int2* upd, int n, unsigned int* s
     if (u.y >= 0) stamp[u.y] = stampValue;
 }
 
+/* requested pages (-2, -3) back to absent */
+__global__ void k_cancel_requests(int* page, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (page[i] < -1) page[i] = -1;
+}
+
 BrickCache::~BrickCache() {
     cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_);
     if (h_tier_) cudaFreeHost(h_tier_);
@@ -99,13 +105,13 @@ void BrickCache::fill_args(DevBricks& b) const {
     b.inc = cfg_.inc; b.vtype = cfg_.vol->vtype; b.stamp = d_stamp_; b.pass = pass_;
 }
 
-void BrickCache::read_brick(uint64_t page, void* dst) const {
+bool BrickCache::read_brick(uint64_t page, void* dst) const {
     const int Lc = cfg_.Lc, sh = cfg_.nLevels - cfg_.Lc;
     const uint64_t msk = (1ull << Lc) - 1;
     int3 m = make_int3((int)((page >> (2 * Lc)) << sh), (int)(((page >> Lc) & msk) << sh), (int)((page & msk) << sh));
     int s[3] = {m.x - cfg_.inc, m.y - cfg_.inc, m.z - cfg_.inc};
     int e[3] = {s[0] + D_, s[1] + D_, s[2] + D_};
-    volume_read_native(cfg_.vol, s, e, dst);
+    return volume_read_native(cfg_.vol, s, e, dst);
 }
 
 int BrickCache::host_threads() const { return cfg_.hostThreads > 0 ? cfg_.hostThreads : omp_get_max_threads(); }
@@ -152,19 +158,41 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
      * thread */
     const int nth = host_threads();
     const int grain = (int)std::max<size_t>(1, std::min<size_t>(8, want / ((size_t)nth * 4)));
-#pragma omp parallel num_threads(nth)
+    std::vector<unsigned char> bad(want, 0);
+    int nbad = 0;
+#pragma omp parallel num_threads(nth) reduction(+ : nbad)
     {
         static thread_local std::vector<unsigned char> stage;
         if (stage.size() < slotBytes_) stage.resize(slotBytes_);
 #pragma omp for schedule(dynamic, grain)
         for (long long k = 0; k < (long long)want; k++) {
             size_t i = miss[k];
-            read_brick(bricks[i], stage.data());
+            if (!read_brick(bricks[i], stage.data())) { bad[k] = 1; nbad++; continue; }
             stream_copy(h_tier_ + (size_t)hslot[i] * slotBytes_, stage.data(), slotBytes_);
         }
         stream_fence();
     }
     msHostRead_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tr).count();
+    if (nbad) {
+        /* a failed read leaves its tier slot empty again: nothing refers to
+         * the brick, and the next request reads it anew */
+        uint64_t first = kEmpty;
+        for (size_t k = 0; k < want; k++) {
+            if (!bad[k]) continue;
+            const size_t i = miss[k];
+            const int hs = hslot[i];
+            if (first == kEmpty) first = bricks[i];
+            hostIndex_[bricks[i] - pageBase_] = -1;
+            hostBrick_[hs] = kEmpty;
+            hostTick_[hs] = 0;
+            freeHost_.push_back(hs);
+            hslot[i] = -1;
+        }
+        hostMisses_ += (int64_t)(want - nbad);
+        *diskLoads += (int64_t)(want - nbad);
+        return fail(VT_ERR_IO, "reading %d brick(s) from the volume failed (first: page %llu)", nbad,
+                    (unsigned long long)first);
+    }
     hostMisses_ += (int64_t)want;
     *diskLoads += (int64_t)want;
     return VT_OK;
@@ -486,6 +514,16 @@ vt_status BrickCache::drop() {
     hostClock_ = 0;
     std::fill(hostTick_.begin(), hostTick_.end(), 0);
     allResident_ = false;
+    return VT_OK;
+}
+
+vt_status BrickCache::cancel_requests(cudaStream_t s) {
+    const unsigned int blocks = (unsigned int)std::min<size_t>(4096, (pageN_ + 255) / 256);
+    launches_++;
+    k_cancel_requests<<<blocks, 256, 0, s>>>(d_page_, pageN_);
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(s));
+    xf_[0].pending = xf_[1].pending = false;
     return VT_OK;
 }
 

@@ -63,6 +63,9 @@ public:
     void fold_stats(vt_stats& st);
     /* empties both tiers (cold cache); no kernel may be in flight */
     vt_status drop();
+    /* pages left requested (-2, -3) by a pass whose requests will not be
+     * serviced (a frame that ended in an error) go back to absent */
+    vt_status cancel_requests(cudaStream_t s);
     void reset_stats();
     int device_slots() const { return nSlots_; }
     /* host copy of a brick's device slot (D^3 voxels); *resident = 0 if none */
@@ -78,7 +81,7 @@ private:
      * buffered, so the next call overlaps it */
     vt_status assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
                             unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync = true);
-    void read_brick(uint64_t code, void* dst) const;
+    bool read_brick(uint64_t code, void* dst) const;
 
     CacheConfig cfg_;
     int D_ = 0, esize_ = 4;

@@ -383,9 +383,22 @@ extern "C" vt_status vt_mlp_forward_noalloc(vt_mlp* m, const float* dev_x, int b
     float* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (g_noalloc_dev[dev]) {
+            /* an address looked up before a cudaDeviceReset belongs to the
+             * destroyed context: the runtime no longer knows it as device
+             * memory of this device, so it is looked up again (a host query,
+             * no allocation) */
+            cudaPointerAttributes pa;
+            if (cudaPointerGetAttributes(&pa, g_noalloc_dev[dev]) != cudaSuccess || pa.type != cudaMemoryTypeDevice ||
+                pa.device != dev) {
+                cudaGetLastError();
+                g_noalloc_dev[dev] = nullptr;
+            }
+        }
         if (!g_noalloc_dev[dev]) {
             /* host code only sees a stand-in for the array: its device address
-             * comes from the runtime, once per device, with that device current */
+             * comes from the runtime, once per device (and context), with
+             * that device current */
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_mlp_noalloc_scratch);
             if (e != cudaSuccess)

@@ -223,15 +223,24 @@ enum { CAND_MISSING = 0, CAND_EMPTY = 1, CAND_HIT = 2 };
 /* Requests page `pidx` once per pass.  A demand request (a ray waits on
  * the brick) moves the page from absent (-1) or speculatively requested
  * (-3) to -2; a speculative one (lookahead) from -1 to -3 and is tagged in
- * the list, so the host loads it only into a slot this frame has not used. */
+ * the list, so the host loads it only into a slot this frame has not used.
+ * Past the list's capacity the page goes back to absent and the request
+ * waits for the next pass (the rays that need it suspend and ask again),
+ * as the reference's per-pass admission cap defers NOCACHED rays
+ * (src/lruCache.cu:184-192). */
 __device__ __forceinline__ void request_brick(const TraceArgs& A, unsigned int pidx, bool spec = false) {
-    int old = atomicCAS(&A.br.page[pidx], -1, spec ? VT_PAGE_SPECULATIVE : VT_PAGE_REQUESTED);
+    const int mark = spec ? VT_PAGE_SPECULATIVE : VT_PAGE_REQUESTED;
+    int old = atomicCAS(&A.br.page[pidx], -1, mark);
     if (old == VT_PAGE_SPECULATIVE && !spec)
         old = atomicCAS(&A.br.page[pidx], VT_PAGE_SPECULATIVE, VT_PAGE_REQUESTED) == VT_PAGE_SPECULATIVE ? -1 : old;
     if (old == -1) {
         unsigned int q = atomicAdd(A.ctl.n_req, 1u);
-        if (q < A.ctl.req_cap) A.ctl.req[q] = pidx | (spec ? VT_REQ_SPECULATIVE : 0ull);
-        else atomicOr(A.ctl.err, VT_KERR_REQUEST_FULL);
+        if (q < A.ctl.req_cap) {
+            A.ctl.req[q] = pidx | (spec ? VT_REQ_SPECULATIVE : 0ull);
+        } else {
+            atomicCAS(&A.br.page[pidx], mark, -1);
+            atomicAdd(&A.ctl.counters[VT_C_REQDEFER], 1ull);
+        }
     }
 }
 
@@ -567,7 +576,8 @@ __device__ int start_ray(const TraceArgs& A, const DevView* sv, unsigned int w, 
     return RAY_DONE;   /* background */
 }
 
-/* count = false: the pixel was counted when a tentative hit was written */
+/* count = false: a tentative hit (past set-aside candidates) is written
+ * uncounted; the hit is counted once, when the pixel is final */
 __device__ __forceinline__ void write_ray(const TraceArgs& A, const DevView* sv, const Ray& R, unsigned int* cnt,
                                           bool count = true) {
     const DevView& V = sv[R.view];
@@ -601,7 +611,9 @@ __device__ __forceinline__ void suspend_ray(const TraceArgs& A, Ray& R, Stk& st,
         for (unsigned int e = 0; e < depth; e++) A.ctl.pool_out[off + nsk + e] = st.e[e];
         rec.depth = depth | (nsk << 8) | ((SKIP && R.tent ? 1u : 0u) << 11); rec.off = off;
     } else {
-        rec.depth = 0; rec.off = 0;   /* pool full: the ray restarts from the root (same result) */
+        /* pool full: the ray restarts from the root and finds the same first
+         * hit; a tentative pixel is rewritten then, and counted once */
+        rec.depth = 0; rec.off = 0;
     }
     A.ctl.out[q] = rec;
     if (SLAB && A.ctl.lookahead > 0) lookahead_requests<VTYPE>(A, R, st, cnt);
@@ -644,11 +656,12 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
         if (w < nItems) {
             int s = start_ray<VTYPE, SKIP>(A, sv, w, R, st, cnt);
             if (s == RAY_RUNNING) s = run_ray<VTYPE, SLAB, U, SKIP>(A, R, st, cnt, -1);
-            if (s == RAY_DONE) write_ray(A, sv, R, cnt, !(SKIP && R.tent));
+            if (s == RAY_DONE) write_ray(A, sv, R, cnt);
             else if (SKIP && s == RAY_TENTATIVE) {
-                write_ray(A, sv, R, cnt);
+                write_ray(A, sv, R, cnt, false);
                 suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt);
             } else if (s == RAY_SUSPENDED) suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt);
+            else if (SKIP && s == RAY_DONE_WRITTEN) cnt[VT_C_HITS]++;   /* the tentative hit stands */
         }
     } else {
         const unsigned int lane = threadIdx.x & 31;
@@ -672,13 +685,13 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
             }
             if (has) {
                 int s = run_ray<VTYPE, SLAB, U, SKIP>(A, R, st, cnt, A.pops);
-                if (s == RAY_DONE) { write_ray(A, sv, R, cnt, !(SKIP && R.tent)); has = false; }
+                if (s == RAY_DONE) { write_ray(A, sv, R, cnt); has = false; }
                 else if (SKIP && s == RAY_TENTATIVE) {
-                    write_ray(A, sv, R, cnt);
+                    write_ray(A, sv, R, cnt, false);
                     suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt);
                     has = false;
                 } else if (s == RAY_SUSPENDED) { suspend_ray<VTYPE, SLAB, SKIP>(A, R, st, cnt); has = false; }
-                else if (SKIP && s == RAY_DONE_WRITTEN) has = false;
+                else if (SKIP && s == RAY_DONE_WRITTEN) { cnt[VT_C_HITS]++; has = false; }   /* the tentative hit stands */
             }
         }
     }

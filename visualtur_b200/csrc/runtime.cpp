@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -208,7 +209,8 @@ static vt_status alloc_ray_buffers(vt_handle* h) {
 }
 
 /* suspended-ray records for `rays` rays and a stack pool of 12 entries per
- * ray on average (rays whose stack does not fit restart from the root) */
+ * ray on average (pool_per_ray; rays whose stack does not fit restart from
+ * the root) */
 static vt_status ensure_suspend_buffers(vt_handle* h, unsigned int rays) {
     if (h->susp_cap >= rays) return VT_OK;
     for (int i = 0; i < 2; i++) {
@@ -220,7 +222,7 @@ static vt_status ensure_suspend_buffers(vt_handle* h, unsigned int rays) {
     rays = (unsigned int)std::min<unsigned long long>(0xFFFFFFFFull,
                                                       std::max<unsigned long long>(rays, h->susp_cap + h->susp_cap / 2ull));
     h->susp_cap = rays;
-    h->pool_cap = (unsigned long long)rays * 12ull;
+    h->pool_cap = (unsigned long long)rays * (unsigned long long)(h->opt.pool_per_ray > 0 ? h->opt.pool_per_ray : 12);
     for (int i = 0; i < 2; i++) {
         CK(cudaMalloc(&h->d_susp[i], (size_t)rays * sizeof(SuspRec)));
         CK(cudaMalloc(&h->d_pool[i], (size_t)h->pool_cap * 8));
@@ -293,6 +295,7 @@ static std::vector<uint64_t> to_pages(const std::vector<uint64_t>& codes, int Lc
 
 static vt_status upload_dense(vt_handle* h) {
     const vt_volume* v = h->vol;
+    if (!v->data) return fail(VT_ERR_UNSUPPORTED, "a resident renderer needs the volume in memory, not a read function");
     h->ve = (long long)(1 << h->nLevels) + 2 * h->P;
     for (int a = 0; a < 3; a++)
         if (v->dims[a] > (1 << h->nLevels)) return fail(VT_ERR_INVALID, "volume larger than the octree");
@@ -336,6 +339,10 @@ extern "C" void vt_default_options(vt_options* o) {
     o->preload = 1;
     o->use_graph = 1;
     o->refine = 0;
+    o->skip = 0;
+    o->max_suspended = 0;
+    o->max_requests = 0;
+    o->pool_per_ray = 0;
 }
 
 static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
@@ -355,6 +362,9 @@ static vt_status validate(const vt_params* p, const vt_octree* o, const vt_optio
             return fail(VT_ERR_INVALID, "unroll must be 1, 2, 4 or 8");
         if (opt->refine < 0 || opt->refine > 16) return fail(VT_ERR_INVALID, "refine must be in 0..16");
         if (opt->skip < 0 || opt->skip > VT_SKIP_MAX) return fail(VT_ERR_INVALID, "skip must be in 0..%d", VT_SKIP_MAX);
+        if (opt->max_passes < 1) return fail(VT_ERR_INVALID, "max_passes must be >= 1");
+        if (opt->max_suspended < 0 || opt->max_requests < 0 || opt->pool_per_ray < 0)
+            return fail(VT_ERR_INVALID, "queue bounds must be >= 0 (0 = default)");
         if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
             return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
     }
@@ -395,6 +405,7 @@ static vt_status init_handle(vt_handle* h) {
         /* a page enters the list at most twice per pass: speculatively, then
          * upgraded to a demand request */
         h->req_cap = (unsigned int)std::max<size_t>(2 * h->leafBricks.size(), 1);
+        if (h->opt.max_requests > 0) h->req_cap = std::min<unsigned int>(h->req_cap, (unsigned int)h->opt.max_requests);
         CK(cudaMalloc(&h->d_req, (size_t)h->req_cap * 8));
     }
     if ((s = alloc_ray_buffers(h)) != VT_OK) return s;
@@ -550,10 +561,11 @@ static vt_status collect_counters(vt_handle* h, cudaStream_t s) {
     st.normal_samples += c[VT_C_NSAMPLES]; st.candidates += c[VT_C_CANDIDATES]; st.expansions += c[VT_C_EXPANSIONS];
     st.device_hits += c[VT_C_DEVHITS]; st.device_misses += c[VT_C_DEVMISSES];
     st.max_stack = std::max<int64_t>(st.max_stack, (int64_t)c[VT_C_MAXSTACK]);
+    st.requests_deferred += c[VT_C_REQDEFER];
     unsigned int err = h->h_ctl->err;
     if (err & VT_KERR_STACK) return fail(VT_ERR_STACK, "a ray's traversal stack overflowed (%d entries)", VT_STACK);
     if (err & VT_KERR_NOTRESIDENT) return fail(VT_ERR_STATE, "resident render met a brick with no slot");
-    if (err & (VT_KERR_SUSPEND_FULL | VT_KERR_REQUEST_FULL)) return fail(VT_ERR_STATE, "demand-paging queue overflow (%u)", err);
+    if (err & VT_KERR_SUSPEND_FULL) return fail(VT_ERR_STATE, "suspended-ray list overflow (more than %u rays waiting on bricks)", h->opt.max_suspended > 0 ? std::min<unsigned int>(h->susp_cap, (unsigned int)h->opt.max_suspended) : h->susp_cap);
     return VT_OK;
 }
 
@@ -606,7 +618,22 @@ static vt_status pass0(vt_handle* h, const TraceArgs& a, int nViews, bool slabMo
 
 struct ViewReq { vt_camera cam; float4* rgba; uint8_t* rgb8; };
 
+static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cudaStream_t s);
+
+/* A frame that ends in an error (a failed brick read, a full queue, the
+ * pass bound) leaves pages its last pass requested but nobody will load:
+ * they go back to absent, so the next frame requests them again. */
 static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream_t s) {
+    vt_status st = render_views_inner(h, vr, n, s);
+    if (st != VT_OK && h->cache && st != VT_ERR_CUDA) {
+        std::string msg = vt_last_error();
+        h->cache->cancel_requests(s);
+        fail(st, "%s", msg.c_str());
+    }
+    return st;
+}
+
+static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cudaStream_t s) {
     auto t0 = std::chrono::steady_clock::now();
     if (n < 1 || n > VT_MAX_VIEWS) return fail(VT_ERR_INVALID, "1..%d views per call", VT_MAX_VIEWS);
     const int tw = h->opt.tile_w, th = h->opt.tile_h;
@@ -629,7 +656,9 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
     const bool allResident = h->opt.resident || h->cache->all_resident();
     vt_status st;
     if (!allResident && (st = ensure_suspend_buffers(h, (unsigned int)real)) != VT_OK) return st;
-    a.ctl.out_cap = h->susp_cap; a.ctl.pool_cap = h->pool_cap;
+    const unsigned int outCap =
+        h->opt.max_suspended > 0 ? std::min<unsigned int>(h->susp_cap, (unsigned int)h->opt.max_suspended) : h->susp_cap;
+    a.ctl.out_cap = outCap; a.ctl.pool_cap = h->pool_cap;
     a.ctl.out = h->d_susp[0]; a.ctl.pool_out = h->d_pool[0];
     if (slabMode) { h->cache->begin_frame(); a.br.pass = h->cache->next_pass(); }
     if ((st = ensure_events(h, 0)) != VT_OK) return st;
@@ -663,11 +692,12 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
             const auto tw = std::chrono::steady_clock::now();
             CK(cudaStreamSynchronize(s));
             wait += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
-            unsigned int nOut = h->h_ctl->n_out, nReq = h->h_ctl->n_req;
+            unsigned int nOut = h->h_ctl->n_out, nReq = std::min(h->h_ctl->n_req, h->req_cap);
             if (nOut == 0) break;
-            if (nOut > h->susp_cap) return fail(VT_ERR_STATE, "suspended-ray list overflow");
-            if (nReq > h->req_cap) return fail(VT_ERR_STATE, "brick request list overflow");
-            if (passes >= h->opt.max_passes) return fail(VT_ERR_TIMEOUT, "frame did not finish in %d passes", passes);
+            if (nOut > outCap)
+                return fail(VT_ERR_STATE, "suspended-ray list overflow (%u rays waiting on bricks, room for %u)", nOut, outCap);
+            if (passes >= h->opt.max_passes)
+                return fail(VT_ERR_TIMEOUT, "frame did not finish in %d passes (max_passes)", passes);
             auto ts = std::chrono::steady_clock::now();
             if ((st = h->cache->service(h->d_req, nReq, s, &h2d)) != VT_OK) return st;
             stall += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ts).count();

@@ -89,7 +89,20 @@ static void read_box(const vt_volume* v, const int s[3], const int e[3], OutT* o
         }
 }
 
-void volume_read(const vt_volume* v, const int s[3], const int e[3], float* out) { read_box(v, s, e, out); }
+static size_t box_voxels(const int s[3], const int e[3]) {
+    size_t n = 1;
+    for (int a = 0; a < 3; a++) n *= (size_t)std::llabs((long long)e[a] - s[a]);
+    return n;
+}
+
+bool volume_read(const vt_volume* v, const int s[3], const int e[3], float* out) {
+    if (!v->reader) { read_box(v, s, e, out); return true; }
+    if (v->vtype == VT_F32) return v->reader(v->user, s, e, out) == 0;
+    std::vector<uint8_t> tmp(box_voxels(s, e));
+    if (v->reader(v->user, s, e, tmp.data()) != 0) return false;
+    for (size_t i = 0; i < tmp.size(); i++) out[i] = (float)tmp[i];
+    return true;
+}
 
 #if defined(__x86_64__)
 void stream_copy(void* dst, const void* src, size_t bytes) {
@@ -102,9 +115,11 @@ void stream_fence() { _mm_sfence(); }
 void stream_copy(void* dst, const void* src, size_t bytes) { memcpy(dst, src, bytes); }
 void stream_fence() {}
 #endif
-void volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out) {
+bool volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out) {
+    if (v->reader) return v->reader(v->user, s, e, out) == 0;
     if (v->vtype == VT_F32) read_box(v, s, e, (float*)out);
     else read_box(v, s, e, (uint8_t*)out);
+    return true;
 }
 
 }  // namespace vtrt
@@ -247,6 +262,21 @@ extern "C" vt_status vt_volume_wrap(const void* data, int vtype, const int64_t d
     return VT_OK;
 }
 
+extern "C" vt_status vt_volume_from_reader(vt_read_fn read, void* user, int vtype, const int64_t dims[3],
+                                           vt_volume** out) {
+    clear_error();
+    if (!read || !dims || !out) return fail(VT_ERR_INVALID, "vt_volume_from_reader: null argument");
+    if (vtype != VT_F32 && vtype != VT_U8) return fail(VT_ERR_INVALID, "bad voxel type %d", vtype);
+    if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0) return fail(VT_ERR_INVALID, "bad dims");
+    vt_volume* v = new vt_volume();
+    v->vtype = vtype;
+    for (int a = 0; a < 3; a++) v->dims[a] = dims[a];
+    v->reader = read;
+    v->user = user;
+    *out = v;
+    return VT_OK;
+}
+
 extern "C" void vt_volume_close(vt_volume* v) {
     if (!v) return;
     if (v->map_base) munmap(v->map_base, v->map_len);
@@ -264,13 +294,19 @@ extern "C" vt_status vt_volume_info(const vt_volume* v, int64_t dims[3], int* vt
 extern "C" vt_status vt_volume_read(const vt_volume* v, const int s[3], const int e[3], float* out) {
     clear_error();
     if (!v || !s || !e || !out) return fail(VT_ERR_INVALID, "vt_volume_read: null argument");
-    volume_read(v, s, e, out);
+    if (!volume_read(v, s, e, out))
+        return fail(VT_ERR_IO, "reading voxels [%d,%d,%d]-[%d,%d,%d) failed", s[0], s[1], s[2], e[0], e[1], e[2]);
     return VT_OK;
 }
 
 extern "C" vt_status vt_volume_read_all(const vt_volume* v, void* out) {
     clear_error();
     if (!v || !out) return fail(VT_ERR_INVALID, "vt_volume_read_all: null argument");
+    if (v->reader) {
+        const int s[3] = {0, 0, 0}, e[3] = {(int)v->dims[0], (int)v->dims[1], (int)v->dims[2]};
+        if (!volume_read_native(v, s, e, out)) return fail(VT_ERR_IO, "reading the whole volume failed");
+        return VT_OK;
+    }
     memcpy(out, v->data, v->voxels() * v->esize());
     return VT_OK;
 }

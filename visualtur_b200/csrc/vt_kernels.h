@@ -14,7 +14,6 @@
 #define VT_KERR_STACK 1u        /* a ray's stack overflowed */
 #define VT_KERR_NOTRESIDENT 2u  /* resident mode met a brick with no slot */
 #define VT_KERR_SUSPEND_FULL 4u /* suspended-ray list overflowed */
-#define VT_KERR_REQUEST_FULL 8u /* brick request list overflowed */
 /* page-table states besides a slot index: -1 absent, and */
 #define VT_PAGE_REQUESTED (-2)     /* a ray waits on the brick */
 #define VT_PAGE_SPECULATIVE (-3)   /* requested ahead of need (lookahead) */
@@ -23,7 +22,7 @@
 /* counter slots in DevCtl::counters */
 enum {
     VT_C_RAYS = 0, VT_C_HITS, VT_C_SAMPLES, VT_C_NSAMPLES, VT_C_CANDIDATES, VT_C_EXPANSIONS,
-    VT_C_MAXSTACK, VT_C_SUSPENDED, VT_C_REQUESTS, VT_C_DEVHITS, VT_C_DEVMISSES, VT_C_COUNT
+    VT_C_MAXSTACK, VT_C_SUSPENDED, VT_C_REQUESTS, VT_C_DEVHITS, VT_C_DEVMISSES, VT_C_REQDEFER, VT_C_COUNT
 };
 
 struct DevCamera {

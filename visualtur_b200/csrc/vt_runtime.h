@@ -34,6 +34,8 @@ struct vt_volume {
     size_t map_len = 0;
     std::vector<unsigned char> owned;
     std::string path;
+    vt_read_fn reader = nullptr;           /* caller's read function (no voxels in memory) */
+    void* user = nullptr;
     size_t esize() const { return vtype == VT_U8 ? 1 : 4; }
     size_t voxels() const { return (size_t)dims[0] * dims[1] * dims[2]; }
 };
@@ -49,10 +51,11 @@ struct vt_octree {
 };
 
 namespace vtrt {
-/* zero-padded hyperslab read, float32 output (FileManager semantics) */
-void volume_read(const vt_volume* v, const int s[3], const int e[3], float* out);
+/* zero-padded hyperslab read, float32 output (FileManager semantics);
+ * false when a reader-backed volume's read failed */
+bool volume_read(const vt_volume* v, const int s[3], const int e[3], float* out);
 /* same, native voxel type, into a buffer of (e-s) voxels */
-void volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out);
+bool volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out);
 /* copies `bytes` (a multiple of 16) to a 16-byte aligned `dst` with stores
  * that bypass the caches (the destination is not read first); the calling
  * thread ends its run of such copies with stream_fence() */
