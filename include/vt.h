@@ -212,6 +212,11 @@ typedef struct {
      * whose stack does not fit the pool of pool_per_ray entries per ray
      * restarts from the root next pass (same pixel). */
     int max_suspended, max_requests, pool_per_ray;
+    /* 1: lookahead requests are queued and their bricks load on a side
+     * stream into never-filled device slots while later passes run (demand
+     * requests never wait for them); 0: they load with the demand requests
+     * of the same service, into slots the frame has not used. */
+    int spec_async;
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -238,9 +243,9 @@ vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], i
 /* Kernel schedule knobs of a live handle (autotuner): ray-tile shape,
  * march unroll, persistent ray queue, traversal steps between refills,
  * persistent CTAs per SM, lookahead requests, graph replay, absent-brick
- * candidates set aside per pass. */
+ * candidates set aside per pass, side-stream lookahead loads. */
 typedef struct {
-    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip;
+    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip, spec_async;
 } vt_tuning;
 vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t);
 vt_status vt_get_tuning(vt_handle* h, vt_tuning* t);
@@ -311,6 +316,7 @@ typedef struct {
     double  ms_fill_wait_total;     /* cumulative host time waiting for device fills to finish */
     double  ms_wait_last_frame;     /* host time of the last frame blocked on its passes' results */
     int64_t requests_deferred;      /* brick requests past max_requests, retried a pass later */
+    int64_t bricks_spec_loaded;     /* lookahead bricks loaded on the side stream (spec_async) */
 } vt_stats;
 vt_status vt_get_stats(vt_handle* h, vt_stats* s);
 /* Empties the brick cache (both tiers): the next frame starts cold.

@@ -50,7 +50,7 @@ class vt_options(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("resident", "tile_w", "tile_h", "unroll", "lookahead", "max_passes",
                                          "host_threads", "record_trace", "trace_level", "record_hits",
                                          "persistent", "blocks_per_sm", "pops", "preload", "use_graph", "refine",
-                                         "skip", "max_suspended", "max_requests", "pool_per_ray")]
+                                         "skip", "max_suspended", "max_requests", "pool_per_ray", "spec_async")]
 
 
 class vt_stats(C.Structure):
@@ -62,7 +62,7 @@ class vt_stats(C.Structure):
         [(n, C.c_double) for n in ("ms_last_frame", "ms_stall_last_frame", "bytes_h2d_last_frame",
                                    "ms_trace_last_frame", "ms_prefetch_last_frame", "ms_host_read_total",
                                    "ms_fill_wait_total", "ms_wait_last_frame")] + \
-        [("requests_deferred", C.c_int64)]
+        [("requests_deferred", C.c_int64), ("bricks_spec_loaded", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -75,7 +75,7 @@ class vt_h5_info(C.Structure):
 
 class vt_tuning(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("tile_w", "tile_h", "unroll", "persistent", "pops", "blocks_per_sm",
-                                         "lookahead", "use_graph", "skip")]
+                                         "lookahead", "use_graph", "skip", "spec_async")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -55,6 +55,14 @@ __global__ void k_cancel_requests(int* page, size_t n) {
 }
 
 BrickCache::~BrickCache() {
+    if (specStream_) cudaStreamSynchronize(specStream_);
+    for (SpecChunk& C : chunks_) {
+        if (C.ev) cudaEventDestroy(C.ev);
+        if (C.hp) cudaFreeHost(C.hp);
+        if (C.hu) cudaFreeHost(C.hu);
+        cudaFree(C.dp); cudaFree(C.du);
+    }
+    if (specStream_) cudaStreamDestroy(specStream_);
     cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_);
     if (h_tier_) cudaFreeHost(h_tier_);
     for (Xfer& X : xf_) {
@@ -97,6 +105,25 @@ vt_status BrickCache::init(const CacheConfig& c) {
     freeHost_.resize(nHost_);
     for (int i = 0; i < nHost_; i++) freeHost_[i] = nHost_ - 1 - i;
     hostTick_.assign(nHost_, 0);
+    slotBusy_.assign(nSlots_, 0);
+    hostBusy_.assign(nHost_, 0);
+    asyncSpec_ = c.asyncSpec;
+    {
+        specMark_.assign(pageN_, 0);
+        specChunkOf_.assign(pageN_, -1);
+        CKC(cudaStreamCreateWithFlags(&specStream_, cudaStreamNonBlocking));
+        chunks_.resize(kSpecChunks);
+        for (int i = 0; i < kSpecChunks; i++) {
+            SpecChunk& C = chunks_[i];
+            C.cap = kSpecChunk;
+            CKC(cudaEventCreateWithFlags(&C.ev, cudaEventDisableTiming));
+            CKC(cudaHostAlloc((void**)&C.hp, C.cap * sizeof(int2), cudaHostAllocDefault));
+            CKC(cudaHostAlloc((void**)&C.hu, C.cap * sizeof(int2), cudaHostAllocDefault));
+            CKC(cudaMalloc(&C.dp, C.cap * sizeof(int2)));
+            CKC(cudaMalloc(&C.du, C.cap * sizeof(int2)));
+            chunkFree_.push_back(kSpecChunks - 1 - i);
+        }
+    }
     return VT_OK;
 }
 
@@ -138,7 +165,7 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
     for (int scanned = 0; scanned < nHost_ && order.size() < want; scanned++) {
         const int hs = hostClock_;
         hostClock_ = hostClock_ + 1 == nHost_ ? 0 : hostClock_ + 1;
-        if (hostBrick_[hs] != kEmpty && hostTick_[hs] < callStart) order.push_back(hs);
+        if (hostBrick_[hs] != kEmpty && hostTick_[hs] < callStart && !hostBusy_[hs]) order.push_back(hs);
     }
     if (order.size() < want) return fail(VT_ERR_STATE, "host tier exhausted");
     for (size_t k = 0; k < want; k++) {
@@ -237,7 +264,7 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
             for (int scanned = 0; scanned < nSlots_ && order.size() < m; scanned++) {
                 const int slot = clock_;
                 clock_ = clock_ + 1 == nSlots_ ? 0 : clock_ + 1;
-                if (slotBrick_[slot] != kEmpty && stampHost_[slot] < lim && mark_[slot] != epoch_) {
+                if (slotBrick_[slot] != kEmpty && stampHost_[slot] < lim && mark_[slot] != epoch_ && !slotBusy_[slot]) {
                     mark_[slot] = epoch_;
                     order.push_back(slot);
                 }
@@ -346,6 +373,35 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
         else demand.push_back(r);
     }
     speculative_ += (int64_t)spec.size();
+    if (asyncSpec_) {
+        /* speculative requests join the side stream's queue; a demand request
+         * for a queued brick takes it out (it loads now), one for a brick in
+         * flight waits for its chunk, one for a brick that landed meanwhile
+         * needs nothing */
+        spec_poll(false);
+        std::vector<int> waitFor;
+        size_t keep = 0;
+        for (size_t i = 0; i < demand.size(); i++) {
+            const uint64_t p = demand[i] - pageBase_;
+            if (specMark_[p] == 2) { waitFor.push_back(specChunkOf_[p]); continue; }
+            if (specMark_[p] == 1) { specMark_[p] = 0; specQueued_--; }
+            if (pageMirror_[p] >= 0) continue;
+            demand[keep++] = demand[i];
+        }
+        demand.resize(keep);
+        std::sort(waitFor.begin(), waitFor.end());
+        waitFor.erase(std::unique(waitFor.begin(), waitFor.end()), waitFor.end());
+        for (int c : waitFor) CKC(cudaStreamWaitEvent(s, chunks_[c].ev, 0));
+        std::sort(spec.begin(), spec.end());
+        for (uint64_t q : spec) {
+            const uint64_t p = q - pageBase_;
+            if (pageMirror_[p] >= 0 || specMark_[p] != 0 || specQueued_ >= (size_t)nSlots_) continue;
+            specMark_[p] = 1;
+            specQ_.push_back(q);
+            specQueued_++;
+        }
+        spec.clear();
+    }
     /* in page order (z fastest): neighbouring bricks share the volume rows
      * of their aprons, so reading them one after another hits the cache */
     std::sort(demand.begin(), demand.end());
@@ -492,12 +548,17 @@ void BrickCache::fold_stats(vt_stats& st) {
     st.bricks_requested = requested_; st.bricks_loaded_disk = hostMisses_;
     st.bricks_loaded_host = hostHits_; st.bricks_prefetched = prefetched_;
     st.bricks_hinted = hinted_; st.bricks_staged = staged_; st.bricks_speculative = speculative_;
+    st.bricks_spec_loaded = specLoaded_;
     st.ms_host_read_total = msHostRead_; st.ms_fill_wait_total = msFillWait_;
     st.launches += launches_ - launchesFolded_;
     launchesFolded_ = launches_;
 }
 vt_status BrickCache::drop() {
     CKC(cudaDeviceSynchronize());
+    spec_poll(true);
+    if (!specMark_.empty()) std::fill(specMark_.begin(), specMark_.end(), 0);
+    if (!specChunkOf_.empty()) std::fill(specChunkOf_.begin(), specChunkOf_.end(), -1);
+    specQ_.clear(); specHead_ = 0; specQueued_ = 0;
     CKC(cudaMemset(d_page_, 0xFF, pageN_ * 4));
     CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
     std::fill(slotBrick_.begin(), slotBrick_.end(), kEmpty);
@@ -517,11 +578,141 @@ vt_status BrickCache::drop() {
     return VT_OK;
 }
 
+void BrickCache::spec_poll(bool wait) {
+    size_t done = 0;
+    for (; done < chunkLive_.size(); done++) {
+        SpecChunk& C = chunks_[chunkLive_[done]];
+        if (wait && done == 0) cudaEventSynchronize(C.ev);   /* the oldest; later ones as they are */
+        else if (cudaEventQuery(C.ev) == cudaErrorNotReady) { cudaGetLastError(); break; }
+        for (size_t i = 0; i < C.pages.size(); i++) {
+            const uint64_t p = C.pages[i] - pageBase_;
+            if (specMark_[p] == 2 && specChunkOf_[p] == chunkLive_[done]) { specMark_[p] = 0; specChunkOf_[p] = -1; }
+            slotBusy_[C.slots[i]] = 0;
+            hostBusy_[C.hslots[i]] = 0;
+        }
+        chunkFree_.push_back(chunkLive_[done]);
+    }
+    chunkLive_.erase(chunkLive_.begin(), chunkLive_.begin() + done);
+}
+
+vt_status BrickCache::spec_issue(const std::vector<uint64_t>& pages, int64_t* loaded) {
+    const int c = chunkFree_.back();
+    chunkFree_.pop_back();
+    SpecChunk& C = chunks_[c];
+    const size_t n = pages.size();
+    std::vector<int> hs;
+    int64_t disk = 0;
+    vt_status st = ensure_host(pages, hs, &disk);
+    if (st != VT_OK) { chunkFree_.push_back(c); return st; }
+    C.pages = pages;
+    C.slots.resize(n);
+    C.hslots = hs;
+    for (size_t i = 0; i < n; i++) {
+        const int slot = freeSlots_.back();
+        freeSlots_.pop_back();
+        const uint64_t p = pages[i] - pageBase_;
+        slotBrick_[slot] = pages[i];
+        pageMirror_[p] = slot;
+        stampHost_[slot] = pass_;
+        slotBusy_[slot] = 1;
+        hostBusy_[hs[i]] = 1;
+        specMark_[p] = 2;
+        specChunkOf_[p] = c;
+        C.slots[i] = slot;
+        C.hp[i] = make_int2(hs[i], slot);
+        C.hu[i] = make_int2((int)p, slot);
+    }
+    /* runs of consecutive host and device slots by the copy engine, the rest
+     * by the fill kernel; then the page entries, after the data */
+    size_t nk = 0;
+    for (size_t k = 0; k < n;) {
+        size_t e = k + 1;
+        while (e < n && C.hp[e].x == C.hp[e - 1].x + 1 && C.hp[e].y == C.hp[e - 1].y + 1) e++;
+        if (e - k >= 16) {
+            CKC(cudaMemcpyAsync((unsigned char*)d_slab_ + (size_t)C.hp[k].y * slotBytes_,
+                                h_tier_ + (size_t)C.hp[k].x * slotBytes_, (e - k) * slotBytes_, cudaMemcpyHostToDevice,
+                                specStream_));
+        } else {
+            for (size_t j = k; j < e; j++) C.hp[nk++] = C.hp[j];
+        }
+        k = e;
+    }
+    if (nk) {
+        launches_++;
+        CKC(cudaMemcpyAsync(C.dp, C.hp, nk * sizeof(int2), cudaMemcpyHostToDevice, specStream_));
+        k_fill_bricks<<<(unsigned int)nk, 256, 0, specStream_>>>((const unsigned char*)d_tier_, slotBytes_, C.dp,
+                                                                  (unsigned char*)d_slab_);
+        CKC(cudaGetLastError());
+    }
+    launches_++;
+    CKC(cudaMemcpyAsync(C.du, C.hu, n * sizeof(int2), cudaMemcpyHostToDevice, specStream_));
+    k_page_update<<<(unsigned int)((n + 255) / 256), 256, 0, specStream_>>>(d_page_, C.du, (int)n, d_stamp_, pass_);
+    CKC(cudaGetLastError());
+    CKC(cudaEventRecord(C.ev, specStream_));
+    chunkLive_.push_back(c);
+    specLoaded_ += (int64_t)n;
+    if (loaded) *loaded += (int64_t)n;
+    return VT_OK;
+}
+
+void BrickCache::set_async_spec(bool on) {
+    if (on == asyncSpec_) return;
+    if (!on) {
+        /* the queue is dropped (its pages stay requested speculatively, so a
+         * ray that needs one asks for it on demand); chunks in flight land */
+        for (size_t i = specHead_; i < specQ_.size(); i++)
+            if (specMark_[specQ_[i] - pageBase_] == 1) specMark_[specQ_[i] - pageBase_] = 0;
+        specQ_.clear(); specHead_ = 0; specQueued_ = 0;
+    }
+    asyncSpec_ = on;
+}
+
+vt_status BrickCache::spec_work(cudaEvent_t passDone, int64_t* loaded) {
+    if (!asyncSpec_) return VT_OK;
+    for (;;) {
+        spec_poll(false);
+        if (specQueued_ == 0 || freeSlots_.empty()) break;
+        if (cudaEventQuery(passDone) != cudaErrorNotReady) break;
+        cudaGetLastError();   /* the query's answer, not a fault */
+        if (chunkFree_.empty()) spec_poll(true);
+        /* next chunk from the queue: entries loaded as demand meanwhile are
+         * gone (mark 0); a never-filled device slot each */
+        std::vector<uint64_t> pages;
+        const size_t want = std::min<size_t>(kSpecChunk, freeSlots_.size());
+        while (specHead_ < specQ_.size() && pages.size() < want) {
+            const uint64_t q = specQ_[specHead_++];
+            const uint64_t p = q - pageBase_;
+            if (specMark_[p] != 1) continue;
+            specMark_[p] = 0;
+            specQueued_--;
+            if (pageMirror_[p] < 0) pages.push_back(q);
+        }
+        if (specHead_ == specQ_.size()) { specQ_.clear(); specHead_ = 0; }
+        if (pages.empty()) continue;
+        /* in page order: neighbouring bricks share the volume rows of their aprons */
+        std::sort(pages.begin(), pages.end());
+        if (spec_issue(pages, loaded) != VT_OK) {
+            /* speculation never fails a frame: the bricks stay requested
+             * speculatively, and a ray that needs one loads it on demand
+             * (where a failed read is reported) */
+            clear_error();
+            break;
+        }
+    }
+    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+    return VT_OK;
+}
+
 vt_status BrickCache::cancel_requests(cudaStream_t s) {
     const unsigned int blocks = (unsigned int)std::min<size_t>(4096, (pageN_ + 255) / 256);
     launches_++;
     k_cancel_requests<<<blocks, 256, 0, s>>>(d_page_, pageN_);
     CKC(cudaGetLastError());
+    /* queued speculative bricks are forgotten with their pages; those in
+     * flight land as usual */
+    for (size_t i = specHead_; i < specQ_.size(); i++)
+        if (specMark_[specQ_[i] - pageBase_] == 1) specMark_[specQ_[i] - pageBase_] = 0;
+    specQ_.clear(); specHead_ = 0; specQueued_ = 0;
     CKC(cudaStreamSynchronize(s));
     xf_[0].pending = xf_[1].pending = false;
     return VT_OK;
@@ -540,7 +731,7 @@ vt_status BrickCache::copy_slot(uint64_t page, void* host, int* resident) {
 }
 
 void BrickCache::reset_stats() {
-    hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = speculative_ = 0;
+    hostHits_ = hostMisses_ = diskLoads_ = requested_ = prefetched_ = hinted_ = staged_ = speculative_ = specLoaded_ = 0;
     msHostRead_ = msFillWait_ = 0;
 }
 

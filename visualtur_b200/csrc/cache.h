@@ -32,6 +32,7 @@ struct CacheConfig {
     const vt_volume* vol = nullptr;
     int nLevels = 0, Lc = 0, inc = 3, edge = 0;
     int deviceSlots = 0, hostSlots = 0, hostThreads = 0;
+    bool asyncSpec = true;   /* lookahead bricks load on a side stream while passes run */
 };
 
 class BrickCache {
@@ -66,6 +67,17 @@ public:
     /* pages left requested (-2, -3) by a pass whose requests will not be
      * serviced (a frame that ended in an error) go back to absent */
     vt_status cancel_requests(cudaStream_t s);
+    /* Speculative (lookahead) bricks, asynchronous mode: service() queues
+     * them instead of loading them; spec_work() loads queued bricks in
+     * chunks on a side stream into never-filled device slots while the
+     * kernel pass behind `passDone` runs, and returns once that pass has
+     * ended (or nothing is left to do).  A demand request for a queued
+     * brick loads it at once; one for a brick in flight makes `s` wait for
+     * its chunk. */
+    vt_status spec_work(cudaEvent_t passDone, int64_t* loaded);
+    void set_async_spec(bool on);
+    bool async_spec() const { return asyncSpec_; }
+    size_t spec_queued() const { return specQueued_; }
     void reset_stats();
     int device_slots() const { return nSlots_; }
     /* host copy of a brick's device slot (D^3 voxels); *resident = 0 if none */
@@ -82,6 +94,9 @@ private:
     vt_status assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
                             unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync = true);
     bool read_brick(uint64_t code, void* dst) const;
+    static constexpr int kSpecChunks = 8;      /* chunks in flight on the side stream */
+    static constexpr size_t kSpecChunk = 512;  /* bricks per chunk: the host reads of one
+                                                  outlast a pass's end by ~0.4 ms at most */
 
     CacheConfig cfg_;
     int D_ = 0, esize_ = 4;
@@ -119,11 +134,32 @@ private:
     } xf_[2];
     int xfNext_ = 0;
     unsigned long long* h_req_ = nullptr; size_t reqCap_ = 0;
+    /* asynchronous speculative loads */
+    struct SpecChunk {
+        cudaEvent_t ev = nullptr;
+        std::vector<uint64_t> pages;
+        std::vector<int> slots, hslots;
+        int2* hp = nullptr; int2* dp = nullptr;   /* (host slot, device slot) pairs */
+        int2* hu = nullptr; int2* du = nullptr;   /* page updates */
+        size_t cap = 0;
+    };
+    vt_status spec_issue(const std::vector<uint64_t>& pages, int64_t* loaded);
+    void spec_poll(bool wait);
+    cudaStream_t specStream_ = nullptr;
+    bool asyncSpec_ = true;
+    std::vector<uint64_t> specQ_;            /* queued pages (FIFO from specHead_) */
+    size_t specHead_ = 0, specQueued_ = 0;
+    std::vector<unsigned char> specMark_;    /* per page: 0, 1 queued, 2 in flight */
+    std::vector<int> specChunkOf_;           /* page in flight -> chunk index */
+    std::vector<SpecChunk> chunks_;          /* ring of chunks (index = issue order % size) */
+    std::vector<int> chunkFree_;             /* chunks not in flight */
+    std::vector<int> chunkLive_;             /* chunks in flight, issue order */
+    std::vector<unsigned char> slotBusy_, hostBusy_;   /* device / host slot read or written in flight */
     unsigned int pass_ = 0, frameStart_ = 1;
     bool allResident_ = false;
     /* stats */
     int64_t hostHits_ = 0, hostMisses_ = 0, diskLoads_ = 0, requested_ = 0, prefetched_ = 0, hinted_ = 0, staged_ = 0,
-            speculative_ = 0;
+            speculative_ = 0, specLoaded_ = 0;
     int64_t launches_ = 0, launchesFolded_ = 0;
     double msHostRead_ = 0, msFillWait_ = 0;
 };

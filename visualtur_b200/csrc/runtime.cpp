@@ -343,6 +343,7 @@ extern "C" void vt_default_options(vt_options* o) {
     o->max_suspended = 0;
     o->max_requests = 0;
     o->pool_per_ray = 0;
+    o->spec_async = 1;
 }
 
 static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
@@ -397,6 +398,7 @@ static vt_status init_handle(vt_handle* h) {
         cc.vol = h->vol; cc.nLevels = h->nLevels; cc.Lc = h->Lc; cc.inc = h->inc; cc.edge = h->edge;
         cc.deviceSlots = p.maxElementsCache; cc.hostSlots = p.maxElementsCache_CPU;
         cc.hostThreads = h->opt.host_threads;
+        cc.asyncSpec = h->opt.spec_async != 0;
         h->cache = new vtrt::BrickCache();
         if ((s = h->cache->init(cc)) != VT_OK) return s;
         if (h->opt.preload && (size_t)p.maxElementsCache >= h->leafBricks.size()) {
@@ -511,6 +513,7 @@ extern "C" vt_status vt_change_cache(vt_handle* h, int nE, const int cDim[3], in
     vtrt::CacheConfig cc;
     cc.vol = h->vol; cc.nLevels = h->nLevels; cc.Lc = h->Lc; cc.inc = h->inc; cc.edge = h->edge;
     cc.deviceSlots = nE; cc.hostSlots = h->p.maxElementsCache_CPU; cc.hostThreads = h->opt.host_threads;
+    cc.asyncSpec = h->opt.spec_async != 0;
     h->cache = new vtrt::BrickCache();
     if ((s = h->cache->init(cc)) != VT_OK) return s;
     if (h->opt.preload && (size_t)nE >= h->leafBricks.size() &&
@@ -685,6 +688,8 @@ static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cuda
         if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();   /* the query's answer, not a fault */
         h->hint.clear();
     }
+    /* queued lookahead bricks load on the cache's side stream while the pass runs */
+    if (slabMode && (st = h->cache->spec_work(h->ev[1], nullptr)) != VT_OK) return st;
     if (!allResident) {
         int cur = 0;
         for (;;) {
@@ -712,6 +717,7 @@ static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cuda
             CK(cudaEventRecord(h->ev[2 * passes + 1], s));
             h->stats.launches++;
             passes++;
+            if ((st = h->cache->spec_work(h->ev[2 * passes - 1], nullptr)) != VT_OK) return st;
         }
     }
     if ((st = collect_counters(h, s)) != VT_OK) return st;
@@ -825,11 +831,13 @@ extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
     o.tile_w = t->tile_w; o.tile_h = t->tile_h; o.unroll = t->unroll; o.persistent = t->persistent;
     o.pops = t->pops; o.blocks_per_sm = t->blocks_per_sm; o.lookahead = t->lookahead; o.use_graph = t->use_graph;
     o.skip = t->skip;
+    o.spec_async = t->spec_async;
     vt_status s = validate(&h->p, h->oct, &o);
     if (s != VT_OK) return s;
     if (o.lookahead < 0 || o.lookahead > 64 || o.pops < 1 || o.blocks_per_sm < 1 || o.blocks_per_sm > 32)
         return fail(VT_ERR_INVALID, "lookahead 0..64, pops >= 1, blocks_per_sm 1..32");
     h->opt = o;
+    if (h->cache) h->cache->set_async_spec(o.spec_async != 0);
     return VT_OK;
 }
 
@@ -840,6 +848,7 @@ extern "C" vt_status vt_get_tuning(vt_handle* h, vt_tuning* t) {
     t->pops = h->opt.pops; t->blocks_per_sm = h->opt.blocks_per_sm; t->lookahead = h->opt.lookahead;
     t->use_graph = h->opt.use_graph;
     t->skip = h->opt.skip;
+    t->spec_async = h->opt.spec_async;
     return VT_OK;
 }
 
