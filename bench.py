@@ -169,21 +169,33 @@ class Clocks:
 
 
 # ----------------------------------------------------------------------------- workload
-def huge_page_array(shape, dtype):
+def huge_page_array(shape, dtype, offset=0):
     """Zero-filled-on-touch host array in anonymous memory advised for
     transparent huge pages (before first touch): random brick reads from a
-    volume of many GB then miss the TLB far less often."""
+    volume of many GB then miss the TLB far less often.  The first element
+    sits `offset` bytes past a page boundary."""
     import ctypes
     import mmap
     nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
-    m = mmap.mmap(-1, nbytes, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
+    m = mmap.mmap(-1, nbytes + 4096, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
     try:
         libc = ctypes.CDLL("libc.so.6")
         addr = ctypes.addressof(ctypes.c_char.from_buffer(m))
-        libc.madvise(ctypes.c_void_p(addr), ctypes.c_size_t(nbytes), 14)   # MADV_HUGEPAGE
+        libc.madvise(ctypes.c_void_p(addr), ctypes.c_size_t(nbytes + 4096), 14)   # MADV_HUGEPAGE
     except (OSError, AttributeError, TypeError):
         pass
-    return m, np.frombuffer(m, dtype).reshape(shape)
+    return m, np.frombuffer(m, dtype, count=int(np.prod(shape)), offset=offset).reshape(shape)
+
+
+def volume_offset(cfg):
+    """Where the host volume starts relative to a cache line: brick boxes
+    start `inc` voxels before a brick boundary (a multiple of 64 bytes of z
+    for 16^3 f32 bricks), so placing the volume `inc` voxels past a line
+    boundary lets each box row begin on a line -- an 88-byte row of a 22^3
+    f32 box then spans 2 cache lines instead of 3 (the reads of the host
+    tier are bound by the lines they touch)."""
+    es = 1 if cfg["gen"] == "fractal" else 4
+    return (cfg["inc"] * es) % 64
 
 
 # Poses of the workloads, as plain numbers: both arms turn them into their
@@ -348,7 +360,7 @@ class Workload:
                                self.octree_path)
         t2 = time.time()
         # host copy of the volume: the out-of-core source and the CPU baseline's input
-        self._host_map, arr = huge_page_array((n * n * n,), np.uint8 if u8 else np.float32)
+        self._host_map, arr = huge_page_array((n * n * n,), np.uint8 if u8 else np.float32, volume_offset(cfg))
         self.host = torch.from_numpy(arr)
         self.host.copy_(dvol)
         torch.cuda.synchronize()
@@ -552,31 +564,17 @@ class Launcher:
         return [(self.bufs[b][1], c.W * c.H * 3) for b, c in enumerate(cams)]
 
     hint_s = 0.0
-    WINDOW = 16      # frames of the scripted path predicted per network call
-
-    @staticmethod
-    def _key(c):
-        return tuple(c.position[:]) + tuple(c.look[:]) + tuple(c.up[:])
 
     def hint(self, cams, f=None):
-        """Predicted bricks of `cams` (frames f, f+1, ...) as the renderer's
-        hint; the network runs once per WINDOW frames of the path."""
+        """The network's prediction for `cams` (this launch's frames and the
+        next launch's) on the device: vt_prefetch_predict requests the
+        predicted absent bricks, which load on the cache's side stream while
+        the launch renders -- no synchronisation or host-side selection."""
         if self.P is None or not cams or self.thr is None:
             return
         t0 = time.perf_counter()
-        from visualtur_b200 import prefetch as pf
-        cache = self.__dict__.setdefault("_probs", {})
-        if any(self._key(c) not in cache for c in cams):
-            win = self.cams(f, max(self.WINDOW, len(cams))) if f is not None else list(cams)
-            win += [c for c in cams if self._key(c) not in {self._key(w) for w in win}]
-            if len(cache) > 4096:
-                cache.clear()
-            probs = self.P.predict(self.torch, np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"])
-                                                         for c in win]))
-            for c, p in zip(win, probs):
-                cache[self._key(c)] = p
-        probs = np.max(np.stack([cache[self._key(c)] for c in cams]), axis=0)
-        self.r.prefetch_hint(self.P.new_bricks_for(probs, self.thr))
+        self.r.prefetch_predict(self.P.mlp, list(cams), self.cfg["n"], self.cfg["fov"], self.thr,
+                                stream=self.stream.cuda_stream)
         self.hint_s += time.perf_counter() - t0
 
     def launch(self, cams, next_cams=(), f=None):
@@ -626,13 +624,11 @@ class ViewLauncher:
     hint_s = 0.0
 
     def hint(self, items):
-        if self.P is None or not items:
+        if self.P is None or not items or self.thr is None:
             return
         t0 = time.perf_counter()
-        from visualtur_b200 import prefetch as pf
-        feats = np.stack([pf.pose_features(c, self.cfg["n"], self.cfg["fov"]) for views in items for c in views])
-        probs = self.P.predict(self.torch, feats).max(axis=0)
-        self.r.prefetch_hint(self.P.new_bricks_for(probs, self.thr))
+        self.r.prefetch_predict(self.P.mlp, [c for views in items for c in views], self.cfg["n"], self.cfg["fov"],
+                                self.thr, stream=self.stream.cuda_stream)
         self.hint_s += time.perf_counter() - t0
 
     def launch(self, items, next_items=(), f=None):
@@ -787,7 +783,8 @@ def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=Fa
 
 # (frames per launch, lookahead, absent-brick candidates a ray may set aside)
 PAGING_CANDIDATES = ((8, 2, 0), (4, 2, 0), (2, 2, 0), (1, 2, 0), (1, 0, 0),
-                     (4, 2, 4), (2, 2, 4), (4, 0, 4), (2, 0, 4), (1, 0, 4))
+                     (8, 0, 0), (4, 0, 0), (2, 0, 0), (4, 1, 0),
+                     (4, 2, 4), (2, 2, 4), (4, 0, 4), (2, 0, 4), (1, 0, 4), (4, 0, 2))
 HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
 VIEWS_PAGING = ((2, 0), (0, 0), (2, 2), (0, 2))                 # batched views: (lookahead, skip)
 
@@ -795,9 +792,9 @@ VIEWS_PAGING = ((2, 0), (0, 0), (2, 2), (0, 2))                 # batched views:
 def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
     """Frames per launch, lookahead, absent-brick candidates set aside per
     pass and the prefetch-hint threshold for an out-of-core fly-through:
-    each candidate renders the same `frames`
-    frames (another stretch of the path than the timed one) from a cold
-    cache; the fastest total device time wins.  Batching more frames per
+    each candidate renders the same `frames` frames (another stretch of the
+    path than the timed one, as long as it) from a cold cache; the fastest
+    total device time wins.  Batching more frames per
     launch amortises launches and host work but needs their joint working
     set in the device cache, and hints help only while the cache has room
     for them -- a small cache thrashes, which only a cold-cache run shows."""
@@ -915,7 +912,10 @@ def run_ours(args, cfg, rank, world, torch, dist):
         paging = {"best": fixed, "table": []}
     elif M["autotune"] and not args.no_autotune and not cfg["resident"] and "views" not in cfg:
         # a stretch of the fly-through away from the timed frames
-        paging, prow = tune_paging(wl, cfg, torch, dev, stream, P, frame0 + args.warmup + args.steps + 97)
+        # as many frames as the timed region, from a cold cache: how much
+        # speculation pays depends on the horizon it is judged over
+        paging, prow = tune_paging(wl, cfg, torch, dev, stream, P, frame0 + args.warmup + args.steps + 97,
+                                   frames=max(args.steps, 8))
         batch = paging["frames_per_launch"]
         paging = {"best": paging, "table": prow}
     if args.skip is not None:
@@ -1071,7 +1071,7 @@ class RefWorkload:
         n = cfg["n"]
         u8 = cfg["gen"] == "fractal"
         t0 = time.time()
-        self._host_map, arr = huge_page_array((n, n, n), np.uint8 if u8 else np.float32)
+        self._host_map, arr = huge_page_array((n, n, n), np.uint8 if u8 else np.float32, volume_offset(cfg))
         host = torch.from_numpy(arr)
         if cfg["gen"] == "sphere":
             c = (n - 1) / 2.0

@@ -220,6 +220,8 @@ typedef struct {
 } vt_options;
 
 typedef struct vt_handle vt_handle;
+/* the learned-prefetch network (vt_mlp_*, below) */
+typedef struct vt_mlp vt_mlp;
 
 void      vt_default_options(vt_options* o);
 /* visualTur::visualTur (src/visualTur.cu:10-35). */
@@ -274,6 +276,23 @@ vt_status vt_get_trace(vt_handle* h, uint32_t* bits, int64_t nwords);
  * of demand, on `stream`; bricks used by the current frame are never
  * evicted.  Returns the number loaded in *loaded (may be NULL). */
 vt_status vt_prefetch(vt_handle* h, const uint64_t* bricks, int64_t n, int64_t* loaded, void* stream);
+
+/* Learned prefetch on the device (no reference counterpart): for the n
+ * poses `cams` (the frames about to be rendered), computes the network's 12
+ * pose features (position relative to the volume centre over `vol_edge`,
+ * look, up, fov_deg / 90, near and far distance to the volume's bounding
+ * sphere over `vol_edge`), runs the network m (its outputs: one probability
+ * per node of an octree level, 8^level of them, level <= levelCubes) and
+ * requests, speculatively, every absent brick holding candidates whose
+ * node's largest probability over the poses exceeds `threshold`.  Work is
+ * enqueued on `stream` (no synchronisation, nothing copied back but the
+ * list of requested bricks); the next vt_render / vt_render_batch queues
+ * those bricks ahead of its lookahead requests, and they load as
+ * spec_async loads them (or as a vt_prefetch_hint when spec_async is 0).
+ * Demand paging stays the fallback: a wrong prediction costs transfers,
+ * never a pixel. */
+vt_status vt_prefetch_predict(vt_handle* h, vt_mlp* m, const vt_camera* cams, int n, float vol_edge, float fov_deg,
+                              float threshold, void* stream);
 
 /* Prefetch hint for the frame after the next vt_render: during that call
  * the bricks' host-tier reads run while its first pass renders (in hint
@@ -331,7 +350,6 @@ vt_status vt_reset_stats(vt_handle* h);
  * BF16 weights, FP32 master weights and FP32 accumulation; He-initialised
  * from `seed`.  Used as pose (12 features) -> per-coarse-node probability
  * that a frame from that pose marches the node. */
-typedef struct vt_mlp vt_mlp;
 vt_status vt_mlp_create(int in, int h1, int h2, int out, uint64_t seed, vt_mlp** m);
 void      vt_mlp_free(vt_mlp* m);
 /* probabilities of `batch` rows of dev_x (batch x in floats) into dev_p */
@@ -345,6 +363,11 @@ vt_status vt_mlp_train_step(vt_mlp* m, const float* dev_x, const float* dev_y, i
  * the weights); synchronises */
 vt_status vt_mlp_gradients(vt_mlp* m, const float* dev_x, const float* dev_y, int batch, float* host_grads,
                            float* loss);
+/* GEMMs on the tensor cores (tcgen05; the default, GEMM inputs rounded to
+ * BF16) or, with on = 0, on the SIMT FMA pipes (FP32 activations) */
+vt_status vt_mlp_use_tensor_cores(vt_mlp* m, int on);
+/* the network's layer widths: in, h1, h2, out */
+vt_status vt_mlp_info(const vt_mlp* m, int dims[4]);
 /* FP32 master weights, layer by layer: W (in x out, row-major) then b */
 vt_status vt_mlp_get_weights(vt_mlp* m, float* host, int64_t* n);
 vt_status vt_mlp_set_weights(vt_mlp* m, const float* host, int64_t n);

@@ -64,7 +64,6 @@ def test_pass_bound_times_out_and_later_frames_finish(workdir, cuda):
             assert err.status == vt.VT_ERR_TIMEOUT
     else:
         pytest.fail("the frame never completed")
-    assert attempt >= 1
     assert_parity(got, oracle_render("c1", workdir))
     r.close()
 

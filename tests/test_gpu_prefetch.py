@@ -90,3 +90,76 @@ def test_learned_prefetch_gains_over_demand_paging(scene, cuda):
     assert lrn["hit_rate"] > dem["hit_rate"]
     assert lrn["stats"]["bricks_requested"] < dem["stats"]["bricks_requested"]
     assert lrn["passes"] < dem["passes"]
+
+
+def test_baseline_network_gains_over_demand_paging(workdir, cuda):
+    """The learned-prefetch configuration itself: the 12 -> 512 -> 512 ->
+    4096 network over level-4 nodes, trained by libvt's kernels with BCE on
+    20 000 (pose, marched-node set) pairs logged by the renderer on random
+    fly-throughs of the 1024^3 blob volume, then judged on a held-out
+    spline fly-through from a cold cache against demand paging alone: the
+    same pixels in every frame, fewer demand misses and passes, a higher
+    device hit rate.  Prediction runs on the device (vt_prefetch_predict):
+    features, forward pass, threshold and the brick requests, with no
+    synchronisation in the frame loop.  Stall times are printed."""
+    import time
+
+    import test_gpu_configs as TC
+    torch = cuda
+    wl = TC.workload("c2s", torch, workdir)
+    cfg = TC.bench.CONFIGS["c2s"]
+    n, fov, lc = cfg["n"], cfg["fov"], cfg["levelC"]
+    # traces: a resident renderer logs the level-4 nodes each pose marches
+    p = vt.make_params(W=240, H=135, octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"], levelCubes=lc,
+                       dimCube=16, distance=cfg["dist"], fov_H=fov, fov_W=fov)
+    tr = vt.visualTur(p, vt.default_options(resident=1, record_trace=1, trace_level=pf.TRACE_LEVEL, record_hits=0),
+                      volume=wl.fm, octree=wl.oc)
+    X, Y = pf.collect_traces(tr, n, 240, 135, fov, np.random.default_rng(7), 100, 200, 1250.0 * n / 1024, 1750.0 * n / 1024,
+                             dist=cfg["dist"])
+    bricks = tr.brick_list()
+    tr.close()
+    assert X.shape == (20000, 12) and Y.shape == (20000, 4096) and 0.01 < Y.mean() < 0.9
+    P = pf.Prefetcher(n, fov, lc, bricks, seed=11)
+    assert P.mlp.dims == (12, 512, 512, 4096)
+    hist = P.train(torch, X, Y, epochs=30, batch=256, lr=1e-3)
+    assert hist[-1] < 0.5 * hist[0]
+
+    pos, tgt = pf.random_flythrough(np.random.default_rng(999), n, 120, 1300.0 * n / 1024, 1700.0 * n / 1024)
+    cams = [pf.look_at(960, 540, cfg["dist"], fov, p_, t_) for p_, t_ in zip(pos, tgt)]
+    stream = torch.cuda.Stream()
+    res = {}
+    for mode in ("demand", "learned"):
+        r = vt.visualTur(wl.params(), vt.default_options(resident=0, preload=0, record_hits=0, persistent=1,
+                                                         lookahead=0, spec_async=1), volume=wl.fm, octree=wl.oc)
+        # frames rendered at 960x540 through batch views (the handle's own size is 1920x1080)
+        out = torch.empty(960 * 540 * 4, dtype=torch.float32, device="cuda")
+        imgs, stall, passes = [], 0.0, 0
+        t0 = time.perf_counter()
+        for k, cam in enumerate(cams):
+            if mode == "learned":
+                r.prefetch_predict(P.mlp, cams[k:k + 4], n, fov, 0.5, stream=stream.cuda_stream)
+            v = vt.vt_view()
+            v.cam, v.dev_rgba, v.dev_rgb8 = cam, out.data_ptr(), None
+            r.render_batch([v], stream=stream.cuda_stream)
+            s = r.stats()
+            stall += s["ms_stall_last_frame"]
+            passes += s["passes"]
+            stream.synchronize()
+            imgs.append(out.cpu().numpy().copy())
+        wall = time.perf_counter() - t0
+        s = r.stats()
+        res[mode] = dict(imgs=imgs, stall=stall / len(cams), passes=passes / len(cams), wall=wall, stats=s,
+                         hit=s["device_hits"] / max(1, s["device_hits"] + s["device_misses"]))
+        r.close()
+    for a, b in zip(res["demand"]["imgs"], res["learned"]["imgs"]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    dem, lrn = res["demand"], res["learned"]
+    print("\nlearned prefetch, held-out 120-frame spline at 960x540 (c2s volume, cold cache):")
+    for k, v in res.items():
+        print("  %-7s stall %.3f ms/frame, passes %.2f/frame, hit rate %.4f, device misses %d, bricks loaded %d, "
+              "predicted %d, wall %.3f s" % (k, v["stall"], v["passes"], v["hit"], v["stats"]["device_misses"],
+                                             v["stats"]["bricks_loaded_disk"], v["stats"]["bricks_hinted"], v["wall"]))
+    assert lrn["stats"]["bricks_spec_loaded"] > 0
+    assert lrn["hit"] > dem["hit"]
+    assert lrn["stats"]["device_misses"] < dem["stats"]["device_misses"]
+    assert lrn["passes"] < dem["passes"]

@@ -145,6 +145,9 @@ _PROTOS = {
     "vt_mlp_get_weights": (C.c_int, [_P, _P, C.POINTER(C.c_int64)]),
     "vt_mlp_set_weights": (C.c_int, [_P, _P, C.c_int64]),
     "vt_mlp_forward_noalloc": (C.c_int, [_P, _P, C.c_int, _P, _P]),
+    "vt_mlp_info": (C.c_int, [_P, C.c_int * 4]),
+    "vt_mlp_use_tensor_cores": (C.c_int, [_P, C.c_int]),
+    "vt_prefetch_predict": (C.c_int, [_P, _P, C.POINTER(vt_camera), C.c_int, C.c_float, C.c_float, C.c_float, _P]),
 }
 
 _lib = None
@@ -526,6 +529,16 @@ class visualTur:
         b = np.ascontiguousarray(bricks, np.uint64)
         check(lib().vt_prefetch_hint(self._h, b.ctypes.data if b.size else None, int(b.size)))
 
+    def prefetch_predict(self, mlp, cams, vol_edge, fov, threshold, stream=None):
+        """Learned prefetch on the device (vt_prefetch_predict): the network
+        `mlp` predicts, from the poses `cams`, the bricks the coming frames
+        march; absent ones are requested speculatively and load while the
+        next render call's passes run.  Nothing is synchronised or copied
+        back to Python."""
+        arr = (vt_camera * len(cams))(*cams)
+        check(lib().vt_prefetch_predict(self._h, mlp._h, arr, len(cams), float(vol_edge), float(fov), float(threshold),
+                                        stream))
+
     def brick_list(self):
         n = C.c_int64(0)
         check(lib().vt_brick_list(self._h, None, C.byref(n)))
@@ -572,6 +585,13 @@ class MLP:
         self.dims = tuple(int(d) for d in dims)
         self._h = C.c_void_p()
         check(lib().vt_mlp_create(*self.dims, seed, C.byref(self._h)))
+
+    def use_tensor_cores(self, on=True):
+        """GEMMs on the tensor cores (default) or on the SIMT FMA pipes."""
+        check(lib().vt_mlp_use_tensor_cores(self._h, 1 if on else 0))
+        self.tensor_cores = bool(on)
+
+    tensor_cores = True
 
     def forward(self, dev_x, batch, dev_p, stream=None):
         check(lib().vt_mlp_forward(self._h, _ptr(dev_x), batch, _ptr(dev_p), stream))

@@ -559,6 +559,7 @@ vt_status BrickCache::drop() {
     if (!specMark_.empty()) std::fill(specMark_.begin(), specMark_.end(), 0);
     if (!specChunkOf_.empty()) std::fill(specChunkOf_.begin(), specChunkOf_.end(), -1);
     specQ_.clear(); specHead_ = 0; specQueued_ = 0;
+    hintQ_.clear(); hintHead_ = 0;
     CKC(cudaMemset(d_page_, 0xFF, pageN_ * 4));
     CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
     std::fill(slotBrick_.begin(), slotBrick_.end(), kEmpty);
@@ -655,6 +656,18 @@ vt_status BrickCache::spec_issue(const std::vector<uint64_t>& pages, int64_t* lo
     return VT_OK;
 }
 
+void BrickCache::spec_hint(const unsigned int* pages, size_t n) {
+    hinted_ += (int64_t)n;
+    for (size_t i = 0; i < n; i++) {
+        const uint64_t q = pageBase_ + pages[i];
+        const uint64_t p = pages[i];
+        if (p >= pageN_ || pageMirror_[p] >= 0 || specMark_[p] == 2) continue;
+        if (specMark_[p] == 0) { specMark_[p] = 1; specQueued_++; }
+        hintQ_.push_back(q);
+        staged_++;
+    }
+}
+
 void BrickCache::set_async_spec(bool on) {
     if (on == asyncSpec_) return;
     if (!on) {
@@ -662,7 +675,10 @@ void BrickCache::set_async_spec(bool on) {
          * ray that needs one asks for it on demand); chunks in flight land */
         for (size_t i = specHead_; i < specQ_.size(); i++)
             if (specMark_[specQ_[i] - pageBase_] == 1) specMark_[specQ_[i] - pageBase_] = 0;
+        for (size_t i = hintHead_; i < hintQ_.size(); i++)
+            if (specMark_[hintQ_[i] - pageBase_] == 1) specMark_[hintQ_[i] - pageBase_] = 0;
         specQ_.clear(); specHead_ = 0; specQueued_ = 0;
+        hintQ_.clear(); hintHead_ = 0;
     }
     asyncSpec_ = on;
 }
@@ -679,6 +695,15 @@ vt_status BrickCache::spec_work(cudaEvent_t passDone, int64_t* loaded) {
          * gone (mark 0); a never-filled device slot each */
         std::vector<uint64_t> pages;
         const size_t want = std::min<size_t>(kSpecChunk, freeSlots_.size());
+        while (hintHead_ < hintQ_.size() && pages.size() < want) {
+            const uint64_t q = hintQ_[hintHead_++];
+            const uint64_t p = q - pageBase_;
+            if (specMark_[p] != 1) continue;
+            specMark_[p] = 0;
+            specQueued_--;
+            if (pageMirror_[p] < 0) pages.push_back(q);
+        }
+        if (hintHead_ == hintQ_.size()) { hintQ_.clear(); hintHead_ = 0; }
         while (specHead_ < specQ_.size() && pages.size() < want) {
             const uint64_t q = specQ_[specHead_++];
             const uint64_t p = q - pageBase_;
@@ -712,7 +737,10 @@ vt_status BrickCache::cancel_requests(cudaStream_t s) {
      * flight land as usual */
     for (size_t i = specHead_; i < specQ_.size(); i++)
         if (specMark_[specQ_[i] - pageBase_] == 1) specMark_[specQ_[i] - pageBase_] = 0;
+    for (size_t i = hintHead_; i < hintQ_.size(); i++)
+        if (specMark_[hintQ_[i] - pageBase_] == 1) specMark_[hintQ_[i] - pageBase_] = 0;
     specQ_.clear(); specHead_ = 0; specQueued_ = 0;
+    hintQ_.clear(); hintHead_ = 0;
     CKC(cudaStreamSynchronize(s));
     xf_[0].pending = xf_[1].pending = false;
     return VT_OK;

@@ -76,6 +76,9 @@ public:
      * its chunk. */
     vt_status spec_work(cudaEvent_t passDone, int64_t* loaded);
     void set_async_spec(bool on);
+    /* pages predicted for the coming frames (already marked requested
+     * speculatively on the device): queued ahead of the lookahead queue */
+    void spec_hint(const unsigned int* pages, size_t n);
     bool async_spec() const { return asyncSpec_; }
     size_t spec_queued() const { return specQueued_; }
     void reset_stats();
@@ -149,6 +152,8 @@ private:
     bool asyncSpec_ = true;
     std::vector<uint64_t> specQ_;            /* queued pages (FIFO from specHead_) */
     size_t specHead_ = 0, specQueued_ = 0;
+    std::vector<uint64_t> hintQ_;            /* predicted pages, loaded before specQ_ */
+    size_t hintHead_ = 0;
     std::vector<unsigned char> specMark_;    /* per page: 0, 1 queued, 2 in flight */
     std::vector<int> specChunkOf_;           /* page in flight -> chunk index */
     std::vector<SpecChunk> chunks_;          /* ring of chunks (index = issue order % size) */

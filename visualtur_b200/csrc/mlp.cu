@@ -4,11 +4,12 @@
  * output per coarse octree node, trained with binary cross-entropy on
  * traces of the nodes each frame marched.
  *
- * Weights are stored in BF16 (what the forward and backward GEMMs read) with
- * FP32 master copies updated by Adam; every GEMM accumulates in FP32.
- * Activations are FP32.  The network is tiny (4.73 MFLOP per pose), so the
- * GEMMs are register-tiled SIMT kernels: inference of one pose per frame is
- * latency-bound and training 20k poses takes well under a second.
+ * Weights are stored in BF16 with FP32 master copies updated by Adam.  The
+ * forward and backward GEMMs run on the tensor cores (tcgen05.mma, BF16 x
+ * BF16 -> FP32 in tensor memory): activations and gradients are kept in
+ * FP32 and rounded to BF16 as they are staged for the MMA.  A register-tiled
+ * SIMT kernel (FP32 activations x BF16 weights, FMA) does the same
+ * contraction where vt_mlp_use_tensor_cores switches the tensor cores off.
  */
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -131,11 +132,174 @@ __global__ void k_to_bf16(const float* w, __nv_bfloat16* wb, long long n) {
         wb[i] = __float2bfloat16_rn(w[i]);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Tensor-core GEMM (tcgen05, sm_100a)                                       */
+/* ------------------------------------------------------------------------ */
+/* The same contraction as k_gemm on the 5th-generation tensor cores: one
+ * 128-thread CTA per 128 x 128 output tile.  Per 64-wide K step the CTA
+ * converts its A and B tiles to BF16 and stores them in shared memory in
+ * the tensor core's K-major, unswizzled layout (core matrices of 8 rows x
+ * 16 bytes; the two 8-element halves of each 16-deep MMA step LBO bytes
+ * apart, successive 8-row groups SBO bytes apart); one thread issues four
+ * tcgen05.mma (M 128, N 128, K 16, BF16 x BF16 -> FP32) into a 128-column
+ * tensor-memory accumulator and commits them to an mbarrier that every
+ * thread waits on before the tiles are overwritten.  The epilogue reads the
+ * accumulator back with tcgen05.ld (warp w owns rows 32w..32w+31), adds the
+ * bias and applies the activation.  Waits are bounded: past the limit the
+ * kernel records VT_MMA_TIMEOUT, frees its tensor memory and returns. */
+#define TC_M 128
+#define TC_N 128
+#define TC_K 64
+#define TC_SMEM (72 * 1024)   /* tiles use 32 KB; 72 KB keeps <= 3 CTAs (384 TMEM columns) per SM */
+
+__device__ unsigned int g_mma_err;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+/* tensor-core shared-memory matrix descriptor: K-major, no swizzle */
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+/* element (row r, k) of a TC_K-deep tile with R rows, in core-matrix order */
+__device__ __forceinline__ int tc_idx(int r, int k, int R) { return (((k >> 3) * (R >> 3) + (r >> 3)) << 6) + ((r & 7) << 3) + (k & 7); }
+
+template <class T> __device__ __forceinline__ __nv_bfloat16 to_bf(T v);
+template <> __device__ __forceinline__ __nv_bfloat16 to_bf<float>(float v) { return __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 to_bf<__nv_bfloat16>(__nv_bfloat16 v) { return v; }
+
+template <class TA, class TB>
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(const TA* A, long long am, long long ak, const TB* B, long long bk,
+                                                    long long bn, float* C, long long cm, int M, int N, int K,
+                                                    const float* bias, int act, int accumulate) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    __nv_bfloat16* sA = (__nv_bfloat16*)tc_smem;                      /* TC_M x TC_K */
+    __nv_bfloat16* sB = (__nv_bfloat16*)(tc_smem + TC_M * TC_K * 2);   /* TC_N x TC_K */
+    unsigned long long* mbar = (unsigned long long*)(tc_smem + (TC_M + TC_N) * TC_K * 2);
+    uint32_t* tslot = (uint32_t*)(mbar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_M, n0 = blockIdx.x * TC_N;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tslot)), "r"(TC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tslot;
+    /* kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
+     * K-major, N / 8 and M / 16 */
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                           ((uint32_t)(TC_M >> 4) << 24);
+    const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int k0 = 0; k0 < K && ok; k0 += TC_K) {
+        /* stage the tiles (zero outside the matrices), walking the operand's
+         * unit-stride dimension across the threads */
+        for (int e = tid; e < TC_M * TC_K; e += 128) {
+            int r, k;
+            if (ak == 1) { r = e / TC_K; k = e % TC_K; } else { k = e / TC_M; r = e % TC_M; }
+            const int m = m0 + r, kk = k0 + k;
+            sA[tc_idx(r, k, TC_M)] = (m < M && kk < K) ? to_bf<TA>(A[(long long)m * am + (long long)kk * ak])
+                                                       : __float2bfloat16_rn(0.0f);
+        }
+        for (int e = tid; e < TC_N * TC_K; e += 128) {
+            int r, k;
+            if (bn == 1) { k = e / TC_N; r = e % TC_N; } else { r = e / TC_K; k = e % TC_K; }
+            const int n = n0 + r, kk = k0 + k;
+            sB[tc_idx(r, k, TC_N)] = (n < N && kk < K) ? to_bf<TB>(B[(long long)kk * bk + (long long)n * bn])
+                                                       : __float2bfloat16_rn(0.0f);
+        }
+        /* the tensor core reads shared memory through the async proxy */
+        asm volatile("fence.proxy.async.shared::cta;");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+            for (int j = 0; j < TC_K / 16; j++) {
+                const uint64_t da = tc_desc(aBase + j * 2 * (TC_M / 8) * 128, (TC_M / 8) * 128, 128);
+                const uint64_t db = tc_desc(bBase + j * 2 * (TC_N / 8) * 128, (TC_N / 8) * 128, 128);
+                const uint32_t accum = (k0 > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                    :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_u32(mbar)));
+        }
+        /* every thread waits for the MMAs: the tiles are reused next step */
+        uint32_t done = 0;
+        for (long long it = 0; it < (1ll << 22) && !done; it++) {
+            asm volatile("{\n\t.reg .pred P1;\n\t"
+                         "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                         "selp.b32 %0, 1, 0, P1;\n\t}"
+                         : "=r"(done) : "r"(smem_u32(mbar)), "r"(phase) : "memory");
+        }
+        if (!done) { atomicOr(&g_mma_err, 1u); ok = false; }
+        phase ^= 1u;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok) {
+        const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TC_N; c0 += 32) {
+            uint32_t v[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const int n = n0 + c0 + j;
+                    if (n >= N) continue;
+                    float x = __uint_as_float(v[j]) + (bias ? bias[n] : 0.0f);
+                    if (accumulate) x += C[(long long)row * cm + n];
+                    if (act == ACT_RELU) x = fmaxf(x, 0.0f);
+                    else if (act == ACT_SIGMOID) x = 1.0f / (1.0f + expf(-x));
+                    C[(long long)row * cm + n] = x;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_N));
+}
+
 static unsigned int g1(long long n) { long long b = (n + 255) / 256; return (unsigned int)(b > 4096 ? 4096 : (b < 1 ? 1 : b)); }
 
 template <class TA, class TB>
-static cudaError_t gemm(const TA* A, long long am, long long ak, const TB* B, long long bk, long long bn, float* C,
-                        long long cm, int M, int N, int K, const float* bias, int act, int acc, cudaStream_t s) {
+static cudaError_t gemm(bool tc, const TA* A, long long am, long long ak, const TB* B, long long bk, long long bn,
+                        float* C, long long cm, int M, int N, int K, const float* bias, int act, int acc, cudaStream_t s) {
+    if (tc) {
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M);
+        k_gemm_tc<TA, TB><<<grid, 128, TC_SMEM, s>>>(A, am, ak, B, bk, bn, C, cm, M, N, K, bias, act, acc);
+        return cudaGetLastError();
+    }
     dim3 grid((N + 63) / 64, (M + 63) / 64);
     k_gemm<TA, TB><<<grid, 256, 0, s>>>(A, am, ak, B, bk, bn, C, cm, M, N, K, bias, act, acc);
     return cudaGetLastError();
@@ -156,7 +320,20 @@ struct vt_mlp {
     float* target = nullptr; float* loss = nullptr;
     int cap = 0;                          /* batch capacity of the activation buffers */
     long long step = 0;
+    bool tc = true;                       /* GEMMs on the tensor cores (tcgen05); false: SIMT FMA */
 };
+
+/* a bounded tensor-core wait gave up (reported by the synchronising calls) */
+static vt_status mma_status() {
+    unsigned int e = 0;
+    if (cudaMemcpyFromSymbol(&e, g_mma_err, sizeof(e)) != cudaSuccess) return vtrt::fail(VT_ERR_CUDA, "MLP status read");
+    if (e) {
+        e = 0;
+        cudaMemcpyToSymbol(g_mma_err, &e, sizeof(e));
+        return vtrt::fail(VT_ERR_TIMEOUT, "a tensor-core GEMM did not complete within its wait bound");
+    }
+    return VT_OK;
+}
 
 static vt_status mlp_buffers(vt_mlp* m, int batch) {
     if (batch <= m->cap) return VT_OK;
@@ -231,7 +408,7 @@ static vt_status forward(vt_mlp* m, const float* x, int batch, cudaStream_t s) {
     const int* d = m->dims;
     CKM(cudaMemcpyAsync(m->act[0], x, (size_t)batch * d[0] * 4, cudaMemcpyDeviceToDevice, s));
     for (int l = 0; l < 3; l++)
-        CKM((gemm<float, __nv_bfloat16>(m->act[l], d[l], 1, m->wb[l], d[l + 1], 1, m->act[l + 1], d[l + 1], batch,
+        CKM((gemm<float, __nv_bfloat16>(m->tc, m->act[l], d[l], 1, m->wb[l], d[l + 1], 1, m->act[l + 1], d[l + 1], batch,
                                        d[l + 1], d[l], m->b[l], l < 2 ? ACT_RELU : ACT_SIGMOID, 0, s)));
     return VT_OK;
 }
@@ -254,12 +431,12 @@ static vt_status backward(vt_mlp* m, const float* y, int batch, cudaStream_t s) 
     k_bce_grad<<<g1(no), 256, 0, s>>>(m->act[3], y, m->dact[3], no, 1.0f / batch, m->loss);
     for (int l = 2; l >= 0; l--) {
         /* gW[l] = act[l]^T dact[l+1]   (d[l] x d[l+1]) */
-        CKM((gemm<float, float>(m->act[l], 1, d[l], m->dact[l + 1], d[l + 1], 1, m->gw[l], d[l + 1], d[l], d[l + 1],
+        CKM((gemm<float, float>(m->tc, m->act[l], 1, d[l], m->dact[l + 1], d[l + 1], 1, m->gw[l], d[l + 1], d[l], d[l + 1],
                                batch, nullptr, ACT_NONE, 0, s)));
         k_colsum<<<(d[l + 1] + 255) / 256, 256, 0, s>>>(m->dact[l + 1], batch, d[l + 1], m->gb[l]);
         if (l > 0) {
             /* dact[l] = dact[l+1] W[l]^T, masked by ReLU */
-            CKM((gemm<float, __nv_bfloat16>(m->dact[l + 1], d[l + 1], 1, m->wb[l], 1, d[l + 1], m->dact[l], d[l], batch,
+            CKM((gemm<float, __nv_bfloat16>(m->tc, m->dact[l + 1], d[l + 1], 1, m->wb[l], 1, d[l + 1], m->dact[l], d[l], batch,
                                            d[l], d[l + 1], nullptr, ACT_NONE, 0, s)));
             k_relu_mask<<<g1((long long)batch * d[l]), 256, 0, s>>>(m->dact[l], m->act[l], (long long)batch * d[l]);
         }
@@ -289,6 +466,7 @@ extern "C" vt_status vt_mlp_train_step(vt_mlp* m, const float* dev_x, const floa
     if (loss) {
         CKM(cudaMemcpyAsync(loss, m->loss, 4, cudaMemcpyDeviceToHost, s));
         CKM(cudaStreamSynchronize(s));
+        return mma_status();
     }
     return VT_OK;
 }
@@ -310,6 +488,20 @@ extern "C" vt_status vt_mlp_gradients(vt_mlp* m, const float* dev_x, const float
         CKM(cudaMemcpy(host_grads + o, m->gb[l], (size_t)m->dims[l + 1] * 4, cudaMemcpyDeviceToHost)); o += m->dims[l + 1];
     }
     if (loss) CKM(cudaMemcpy(loss, m->loss, 4, cudaMemcpyDeviceToHost));
+    return mma_status();
+}
+
+extern "C" vt_status vt_mlp_use_tensor_cores(vt_mlp* m, int on) {
+    vtrt::clear_error();
+    if (!m) return vtrt::fail(VT_ERR_INVALID, "null argument");
+    m->tc = on != 0;
+    return VT_OK;
+}
+
+extern "C" vt_status vt_mlp_info(const vt_mlp* m, int dims[4]) {
+    vtrt::clear_error();
+    if (!m || !dims) return vtrt::fail(VT_ERR_INVALID, "null argument");
+    memcpy(dims, m->dims, sizeof(m->dims));
     return VT_OK;
 }
 
@@ -412,11 +604,11 @@ extern "C" vt_status vt_mlp_forward_noalloc(vt_mlp* m, const float* dev_x, int b
     float* h2 = scratch + (size_t)batch * d[1];
     /* every activation element is written before it is read, so the array's
      * leftovers from the previous call need no clearing */
-    CKM((gemm<float, __nv_bfloat16>(dev_x, d[0], 1, m->wb[0], d[1], 1, h1, d[1], batch, d[1], d[0], m->b[0],
+    CKM((gemm<float, __nv_bfloat16>(m->tc, dev_x, d[0], 1, m->wb[0], d[1], 1, h1, d[1], batch, d[1], d[0], m->b[0],
                                     ACT_RELU, 0, s)));
-    CKM((gemm<float, __nv_bfloat16>(h1, d[1], 1, m->wb[1], d[2], 1, h2, d[2], batch, d[2], d[1], m->b[1],
+    CKM((gemm<float, __nv_bfloat16>(m->tc, h1, d[1], 1, m->wb[1], d[2], 1, h2, d[2], batch, d[2], d[1], m->b[1],
                                     ACT_RELU, 0, s)));
-    CKM((gemm<float, __nv_bfloat16>(h2, d[2], 1, m->wb[2], d[3], 1, dev_p, d[3], batch, d[3], d[2], m->b[2],
+    CKM((gemm<float, __nv_bfloat16>(m->tc, h2, d[2], 1, m->wb[2], d[3], 1, dev_p, d[3], batch, d[3], d[2], m->b[2],
                                     ACT_SIGMOID, 0, s)));
     return VT_OK;
 }

@@ -802,9 +802,42 @@ __global__ void k_fill_dense(void* dst, const void* src, long long nx, long long
     }
 }
 
+/* Learned prefetch: one thread per leaf brick (page index); its coarse
+ * node at `level` is the brick's coordinates shifted by levelCubes - level,
+ * Morton-ordered like the trace log's bits.  Absent pages of predicted
+ * nodes go to -3 (requested speculatively) and into the list; past the
+ * list's capacity a page goes back to absent. */
+__global__ void k_predict_requests(int* page, const unsigned int* leafPages, int nLeaf, const float* probs, int ncams,
+                                   int level, int Lc, float thr, unsigned int* list, unsigned int* count,
+                                   unsigned int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nLeaf) return;
+    const unsigned int p = leafPages[i];
+    const unsigned int m = (1u << Lc) - 1u, sh = (unsigned int)(Lc - level);
+    const unsigned int bx = p >> (2 * Lc), by = (p >> Lc) & m, bz = p & m;
+    const unsigned long long node = (spread3(bx >> sh) << 2) | (spread3(by >> sh) << 1) | spread3(bz >> sh);
+    const long long nodes = 1ll << (3 * level);
+    float pm = 0.0f;
+    for (int c = 0; c < ncams; c++) pm = fmaxf(pm, __ldg(probs + (long long)c * nodes + (long long)node));
+    if (!(pm > thr) || page[p] != -1) return;
+    if (atomicCAS(&page[p], -1, VT_PAGE_SPECULATIVE) != -1) return;
+    const unsigned int q = atomicAdd(count, 1u);
+    if (q < cap) list[q] = p;
+    else atomicCAS(&page[p], VT_PAGE_SPECULATIVE, -1);
+}
+
 }  // namespace vt
 
 using namespace vt;
+
+cudaError_t vt_launch_predict_requests(int* page, const unsigned int* leafPages, int nLeaf, const float* probs,
+                                       int ncams, int level, int Lc, float thr, unsigned int* list,
+                                       unsigned int* count, unsigned int cap, cudaStream_t s) {
+    if (nLeaf <= 0) return cudaSuccess;
+    k_predict_requests<<<(nLeaf + 255) / 256, 256, 0, s>>>(page, leafPages, nLeaf, probs, ncams, level, Lc, thr, list,
+                                                          count, cap);
+    return cudaGetLastError();
+}
 
 cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, bool persistent, int blocksPerSM, cudaStream_t s) {
     const int threads = 128;

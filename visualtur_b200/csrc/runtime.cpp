@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -185,6 +186,11 @@ struct vt_handle {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t s_int = nullptr;
     std::vector<uint64_t> hint;            /* bricks to load for the next frame */
+    /* learned prefetch on the device (vt_prefetch_predict) */
+    unsigned int* d_leafPages = nullptr; int nLeaf = 0;
+    float* d_feat = nullptr; float* h_feat = nullptr; float* d_probs = nullptr; int predCap = 0; int probsCap = 0;
+    unsigned int* d_pred = nullptr; unsigned int* h_pred = nullptr;   /* [0] = count, then pages */
+    cudaEvent_t predDone = nullptr; bool predPending = false;
     vt_stats stats;
     bool lastValid = false;
 };
@@ -459,6 +465,10 @@ extern "C" void vt_destroy(vt_handle* h) {
     if (h->h_views) cudaFreeHost(h->h_views);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    cudaFree(h->d_leafPages); cudaFree(h->d_feat); cudaFree(h->d_probs); cudaFree(h->d_pred);
+    if (h->h_feat) cudaFreeHost(h->h_feat);
+    if (h->h_pred) cudaFreeHost(h->h_pred);
+    if (h->predDone) cudaEventDestroy(h->predDone);
     if (h->s_int) cudaStreamDestroy(h->s_int);
     delete h->cache;
     if (h->ownVol) vt_volume_close(h->vol);
@@ -688,6 +698,18 @@ static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cuda
         if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();   /* the query's answer, not a fault */
         h->hint.clear();
     }
+    /* bricks the network predicted for these frames join the side stream's
+     * queue ahead of the lookahead requests */
+    if (slabMode && h->predPending) {
+        h->predPending = false;
+        CK(cudaEventSynchronize(h->predDone));
+        const unsigned int np = std::min<unsigned int>(h->h_pred[0], (unsigned int)h->nLeaf);
+        if (h->cache->async_spec()) {
+            h->cache->spec_hint(h->h_pred + 1, np);
+        } else {
+            h->hint.assign(h->h_pred + 1, h->h_pred + 1 + np);
+        }
+    }
     /* queued lookahead bricks load on the cache's side stream while the pass runs */
     if (slabMode && (st = h->cache->spec_work(h->ev[1], nullptr)) != VT_OK) return st;
     if (!allResident) {
@@ -864,6 +886,77 @@ extern "C" vt_status vt_prefetch_hint(vt_handle* h, const uint64_t* bricks, int6
     return VT_OK;
 }
 
+extern "C" vt_status vt_prefetch_predict(vt_handle* h, vt_mlp* m, const vt_camera* cams, int n, float vol_edge,
+                                         float fov_deg, float threshold, void* stream) {
+    clear_error();
+    if (!h || !m || !cams || n < 1 || vol_edge <= 0) return fail(VT_ERR_INVALID, "vt_prefetch_predict: bad arguments");
+    if (h->opt.resident || !h->cache) return VT_OK;
+    int d[4];
+    vt_status st = vt_mlp_info(m, d);
+    if (st != VT_OK) return st;
+    int level = 0;
+    while (level < 10 && (1 << (3 * level)) < d[3]) level++;
+    if (d[0] != 12 || (1 << (3 * level)) != d[3] || level > h->Lc)
+        return fail(VT_ERR_INVALID, "the network must map 12 pose features to 8^level outputs, level <= levelCubes (%d)",
+                    h->Lc);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!h->d_leafPages) {
+        std::vector<unsigned int> pages(h->leafBricks.size());
+        for (size_t i = 0; i < pages.size(); i++) pages[i] = (unsigned int)code_to_page(h->leafBricks[i], h->Lc);
+        h->nLeaf = (int)pages.size();
+        CK(cudaMalloc(&h->d_leafPages, std::max<size_t>(1, pages.size()) * 4));
+        CK(cudaMemcpy(h->d_leafPages, pages.data(), pages.size() * 4, cudaMemcpyHostToDevice));
+        CK(cudaMalloc(&h->d_pred, ((size_t)h->nLeaf + 1) * 4));
+        CK(cudaHostAlloc(&h->h_pred, ((size_t)h->nLeaf + 1) * 4, cudaHostAllocDefault));
+        CK(cudaEventCreateWithFlags(&h->predDone, cudaEventDisableTiming));
+    }
+    if (h->predPending) CK(cudaEventSynchronize(h->predDone));   /* its buffers are reused */
+    if (n > h->predCap) {
+        cudaFree(h->d_feat);
+        if (h->h_feat) cudaFreeHost(h->h_feat);
+        h->d_feat = nullptr; h->h_feat = nullptr;
+        CK(cudaMalloc(&h->d_feat, (size_t)n * 12 * 4));
+        CK(cudaHostAlloc(&h->h_feat, (size_t)n * 12 * 4, cudaHostAllocDefault));
+        h->predCap = n;
+    }
+    if ((long long)n * d[3] > h->probsCap) {
+        cudaFree(h->d_probs);
+        h->d_probs = nullptr;
+        CK(cudaMalloc(&h->d_probs, (size_t)n * d[3] * 4));
+        h->probsCap = n * d[3];
+    }
+    /* pose features, as the network was trained on them */
+    const double c = (vol_edge - 1.0) / 2.0, rad = std::sqrt(3.0) * vol_edge / 2.0;
+    for (int k = 0; k < n; k++) {
+        float* f = h->h_feat + 12 * k;
+        const vt_camera& cm = cams[k];
+        double dd = 0;
+        for (int a = 0; a < 3; a++) {
+            const double r = (double)cm.position[a] - c;
+            f[a] = (float)(r / vol_edge);
+            dd += r * r;
+            f[3 + a] = cm.look[a];
+            f[6 + a] = cm.up[a];
+        }
+        dd = std::sqrt(dd);
+        f[9] = (float)(fov_deg / 90.0);
+        f[10] = (float)(std::max(dd - rad, 0.0) / vol_edge);
+        f[11] = (float)((dd + rad) / vol_edge);
+    }
+    CK(cudaMemcpyAsync(h->d_feat, h->h_feat, (size_t)n * 12 * 4, cudaMemcpyHostToDevice, s));
+    if ((st = vt_mlp_forward(m, h->d_feat, n, h->d_probs, stream)) != VT_OK) return st;
+    CK(cudaMemsetAsync(h->d_pred, 0, 4, s));
+    DevBricks b;
+    h->cache->fill_args(b);
+    CK(vt_launch_predict_requests(b.page, h->d_leafPages, h->nLeaf, h->d_probs, n, level, h->Lc, threshold,
+                                  h->d_pred + 1, h->d_pred, (unsigned int)h->nLeaf, s));
+    h->stats.launches++;
+    CK(cudaMemcpyAsync(h->h_pred, h->d_pred, ((size_t)h->nLeaf + 1) * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(h->predDone, s));
+    h->predPending = true;
+    return VT_OK;
+}
+
 extern "C" vt_status vt_brick_list(vt_handle* h, uint64_t* bricks, int64_t* n) {
     clear_error();
     if (!h || !n) return fail(VT_ERR_INVALID, "null argument");
@@ -885,6 +978,7 @@ extern "C" vt_status vt_drop_cache(vt_handle* h) {
     clear_error();
     if (!h) return fail(VT_ERR_INVALID, "null handle");
     h->hint.clear();
+    if (h->predPending) { cudaEventSynchronize(h->predDone); h->predPending = false; }
     if (!h->cache) return VT_OK;
     return h->cache->drop();
 }

@@ -130,5 +130,10 @@ cudaError_t vt_launch_trace(const TraceArgs& a, bool slab, bool persistent, int 
 cudaError_t vt_launch_rays(const DevCamera& c, float* dirs, cudaStream_t s);
 cudaError_t vt_launch_cube(const DevCamera& c, const float* cube, int3 minBox, int3 cubeDim,
                            int3 cubeInc, float iso, float3 light, float4* rgba, cudaStream_t s);
+/* learned prefetch: speculative requests of the leaf bricks whose coarse
+ * node (at `level`) has a largest probability over `ncams` rows above thr */
+cudaError_t vt_launch_predict_requests(int* page, const unsigned int* leafPages, int nLeaf, const float* probs,
+                                       int ncams, int level, int Lc, float thr, unsigned int* list,
+                                       unsigned int* count, unsigned int cap, cudaStream_t s);
 cudaError_t vt_launch_fill_dense(void* dst, int vtype, const void* src, long long nx, long long ny,
                                  long long nz, int P, long long ey, long long ez, cudaStream_t s);
