@@ -68,7 +68,11 @@ def test_mlp_gradients_match_cpu(dims, batch, tc, cuda):
     dp = torch.empty(batch * dims[3], dtype=torch.float32, device="cuda")
     m.forward(dx, batch, dp)
     torch.cuda.synchronize()
-    assert np.abs(dp.cpu().numpy().reshape(batch, -1) - p).max() < 1e-4
+    # probabilities: FP32 activations agree to summation order (1e-4); on the
+    # tensor cores an activation within an FP32 rounding of a BF16 rounding
+    # boundary can round to the neighbouring BF16 value on one side only,
+    # which moves an output by up to a few 1e-4 (bar 2e-3)
+    assert np.abs(dp.cpu().numpy().reshape(batch, -1) - p).max() < (2e-3 if tc else 1e-4)
 
 
 @pytest.mark.parametrize("tc", [True, False])
