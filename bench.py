@@ -522,12 +522,15 @@ def cpu_baseline(cfg, wl, octree_path, budget_s, nthreads=0, step=0, octree=None
 
 
 def oracle_mismatch(product_rgba, oracle):
-    """Rays of the oracle's sample whose product RGBA differs in any bit."""
+    """Rays of the oracle's sample whose product RGBA differs in any bit; a
+    NaN colour (a 0/0 refinement on integer voxels, on both sides) counts as
+    equal to a NaN, whatever the NaN's bits."""
     out, stride = oracle
-    a = product_rgba[::stride].view(np.uint32)
-    b = out["rgba"][::stride].view(np.uint32)
-    return {"oracle_checked_rays": int(a.shape[0]), "oracle_mismatch_rays": int((a != b).any(axis=1).sum()),
-            "oracle_hits": int((out["node"][::stride] != 0).sum())}
+    pa, pb = product_rgba[::stride], out["rgba"][::stride]
+    nan_a, nan_b = np.isnan(pa), np.isnan(pb)
+    diff = (pa.view(np.uint32) != pb.view(np.uint32)) & ~(nan_a & nan_b)
+    return {"oracle_checked_rays": int(pa.shape[0]), "oracle_mismatch_rays": int(diff.any(axis=1).sum()),
+            "oracle_nan_rays": int(nan_b.any(axis=1).sum()), "oracle_hits": int((out["node"][::stride] != 0).sum())}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -965,6 +968,25 @@ def run_ours(args, cfg, rank, world, torch, dist):
     # oracle comparison of the CPU baseline's ray sample
     product_sample = product_frame_rgba(wl.vt, wl.r, vt_cam(wl.vt, cfg, sample_pose(cfg, frame0 + args.warmup)),
                                         torch, dev, stream)
+    # with hints on, the same timed stretch with them off: what the learned
+    # prefetch gains on this workload (stall, device-cache hit rate, time)
+    learned_gain = None
+    if P is not None and getattr(L, "thr", None) is not None and "views" not in cfg:
+        thr = L.thr
+        L.thr = None
+        offms, offper, _, _ = timed_frames(L, frame0, args.warmup, args.steps, dist, label="hints_off")
+        L.thr = thr
+        so = wl.r.stats()
+        learned_gain = {
+            "hint_threshold": thr,
+            "ms_per_step_on": round(t_max / args.steps, 4),
+            "ms_per_step_off": round(max_over_ranks(dist, torch, sum(offms), dev) / args.steps, 4),
+            "stall_ms_per_step_on": round(sum(x["ms_stall_last_frame"] for x in per) / args.steps, 4),
+            "stall_ms_per_step_off": round(sum(x["ms_stall_last_frame"] for x in offper) / args.steps, 4),
+            "device_hit_rate_on": round(st["device_hits"] / max(1, st["device_hits"] + st["device_misses"]), 5),
+            "device_hit_rate_off": round(so["device_hits"] / max(1, so["device_hits"] + so["device_misses"]), 5),
+            "passes_per_launch_on": round(sum(x["passes"] for x in per) / len(per), 3),
+            "passes_per_launch_off": round(sum(x["passes"] for x in offper) / len(offper), 3)}
     # the plain LRU renderer on the same steps, for comparison
     plain = None
     check = None
@@ -1038,7 +1060,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
             plain["same_pixels"] = check["best"] == check["plain"]
             plain["pixels_checked_frames"] = check["frames"]
     if P is not None:
-        line["learned_prefetch"] = wl.train_info
+        line["learned_prefetch"] = dict(wl.train_info, **({"timed_gain": learned_gain} if learned_gain else {}))
     if tune:
         line["autotune"] = {"best": tune["best"], "points": tune["points"]}
         if paging:

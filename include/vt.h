@@ -217,6 +217,14 @@ typedef struct {
      * requests never wait for them); 0: they load with the demand requests
      * of the same service, into slots the frame has not used. */
     int spec_async;
+    /* 0: one trace kernel per pass (traversal and march fused); k in 1..8:
+     * wavefront passes -- k rounds of a traversal kernel that queues each
+     * ray's next resident candidate, binned by brick, and a march kernel
+     * that stages each binned brick into shared memory with one bulk copy
+     * and marches its rays from there; then the fused kernel finishes the
+     * rays still waiting.  Same image.  Slab mode, in-order traversal
+     * (skip 0) only. */
+    int wavefront;
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -245,9 +253,10 @@ vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], i
 /* Kernel schedule knobs of a live handle (autotuner): ray-tile shape,
  * march unroll, persistent ray queue, traversal steps between refills,
  * persistent CTAs per SM, lookahead requests, graph replay, absent-brick
- * candidates set aside per pass, side-stream lookahead loads. */
+ * candidates set aside per pass, side-stream lookahead loads, wavefront
+ * rounds. */
 typedef struct {
-    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip, spec_async;
+    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip, spec_async, wavefront;
 } vt_tuning;
 vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t);
 vt_status vt_get_tuning(vt_handle* h, vt_tuning* t);

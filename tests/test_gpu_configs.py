@@ -8,7 +8,7 @@ the 2048^3 uint8 fractal with 32^3 bricks.  Each is generated on the device
 by libvt's seeded generators, its octree built by libvt's GPU builder, and
 rendered through vt_render from a cold brick cache with the product's
 settings (persistent ray queue, lookahead requests, with and without
-set-aside candidates); the oracle renders the same frames from the same
+set-aside candidates, fused and wavefront passes); the oracle renders the same frames from the same
 volume and octree.  Bar: hit node and brick ids bit-exact, t within 1e-3
 voxel, normals within 1e-3 rad, RGB8 within 1 LSB (and in fact every RGBA
 bit equal).  The oracle's own CPU builder must write the same octree file
@@ -97,8 +97,8 @@ def check_blobs(name, cuda, workdir):
     cfg = bench.CONFIGS[name]
     wl = workload(name, cuda, workdir)
     assert wl.oc.nLevels == int(math.log2(cfg["n"])) and wl.brick == 16
-    for skip in (0, 2):
-        for cam, got in product_frames(wl, cfg, [0, 37], skip=skip, **BEST):
+    for skip, wave in ((0, 0), (2, 0), (0, 2)):
+        for cam, got in product_frames(wl, cfg, [0, 37], skip=skip, wavefront=wave, **BEST):
             want = oracle_frame(wl, cfg, cam)
             assert_parity(got, want)
             assert want["agg"]["hits"] > 100000
@@ -130,8 +130,8 @@ def test_u8_fractal_frames(workdir, cuda):
     cfg = bench.CONFIGS["c5s"]
     wl = workload("c5s", cuda, workdir)
     assert wl.volume.dtype == np.uint8 and wl.brick == 32
-    for skip in (0, 2):
-        for cam, got in product_frames(wl, cfg, [0, 211], skip=skip, **BEST):
+    for skip, wave in ((0, 0), (2, 0), (0, 3)):
+        for cam, got in product_frames(wl, cfg, [0, 211], skip=skip, wavefront=wave, **BEST):
             want = oracle_frame(wl, cfg, cam)
             assert_parity(got, want)
             assert want["agg"]["hits"] > 100000

@@ -34,8 +34,10 @@ def product_render(case, workdir, mode, vol=None, extra_ops=(), refine=0):
         dev, host = 24, 16
     opt = vt.default_options(resident=1 if mode in ("resident", "persist") else 0, record_hits=1,
                              persistent=1 if mode in ("persist", "demand_la", "demand_skip") else 0,
-                             lookahead={"demand_la": 3, "demand_skip": 2, "demand_la_sync": 3}.get(mode, 0), pops=3,
+                             lookahead={"demand_la": 3, "demand_skip": 2, "demand_la_sync": 3,
+                                        "demand_wave": 2}.get(mode, 0), pops=3,
                              spec_async=0 if mode == "demand_la_sync" else 1,
+                             wavefront={"wave": 2, "demand_wave": 3, "wave1": 1}.get(mode, 0),
                              unroll={"persist": 4, "demand_la": 2, "slab": 8}.get(mode, 1), refine=refine,
                              skip={"demand_skip": 4, "demand_skip_np": 2}.get(mode, 0))
     p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=c["levelO"],
@@ -92,7 +94,7 @@ def assert_parity(a, b):
 
 
 @pytest.mark.parametrize("mode", ["resident", "slab", "demand", "persist", "demand_la", "demand_la_sync",
-                                  "demand_skip", "demand_skip_np"])
+                                  "demand_skip", "demand_skip_np", "wave", "wave1", "demand_wave"])
 @pytest.mark.parametrize("case", sorted(F.CASES))
 def test_render_parity(case, mode, workdir, cuda):
     a = product_render(case, workdir, mode)

@@ -23,8 +23,12 @@
 namespace vt {
 
 /* ---- samplers: voxel at brick-relative integer coordinates ------------- */
-template <int VTYPE>
+template <int VTYPE, bool SHM = false>
 __device__ __forceinline__ float ldv(const void* p, long long i) {
+    if (SHM) {   /* a brick staged in shared memory */
+        if (VTYPE == 0) return ((const float*)p)[i];
+        return (float)((const unsigned char*)p)[i];
+    }
     if (VTYPE == 0) return __ldg((const float*)p + i);
     return (float)__ldg((const unsigned char*)p + i);
 }
@@ -39,7 +43,7 @@ struct Samp {
 };
 
 /* getElementInterpolate (src/rayCaster.cu:86-106). */
-template <int VTYPE, bool SLAB = false>
+template <int VTYPE, bool SLAB = false, bool SHM = false>
 __device__ __forceinline__ float interp(const Samp& s, float3 p) {
     float rx, ry, rz;
     float px = modff(p.x, &rx), py = modff(p.y, &ry), pz = modff(p.z, &rz);
@@ -50,10 +54,10 @@ __device__ __forceinline__ float interp(const Samp& s, float3 p) {
         /* a brick holds < 2^31 voxels: 32-bit index arithmetic */
         const int sx = (int)s.sx, sy = (int)s.sy;
         const int b = x0 * sx + y0 * sy + z0;
-        v000 = ldv<VTYPE>(s.base, b); v001 = ldv<VTYPE>(s.base, b + 1);
-        v010 = ldv<VTYPE>(s.base, b + sy); v011 = ldv<VTYPE>(s.base, b + sy + 1);
-        v100 = ldv<VTYPE>(s.base, b + sx); v101 = ldv<VTYPE>(s.base, b + sx + 1);
-        v110 = ldv<VTYPE>(s.base, b + sx + sy); v111 = ldv<VTYPE>(s.base, b + sx + sy + 1);
+        v000 = ldv<VTYPE, SHM>(s.base, b); v001 = ldv<VTYPE, SHM>(s.base, b + 1);
+        v010 = ldv<VTYPE, SHM>(s.base, b + sy); v011 = ldv<VTYPE, SHM>(s.base, b + sy + 1);
+        v100 = ldv<VTYPE, SHM>(s.base, b + sx); v101 = ldv<VTYPE, SHM>(s.base, b + sx + 1);
+        v110 = ldv<VTYPE, SHM>(s.base, b + sx + sy); v111 = ldv<VTYPE, SHM>(s.base, b + sx + sy + 1);
     } else {
         const long long b = (long long)x0 * s.sx + (long long)y0 * s.sy + z0;
         v000 = ldv<VTYPE>(s.base, b); v001 = ldv<VTYPE>(s.base, b + 1);
@@ -72,7 +76,7 @@ __device__ __forceinline__ float interp(const Samp& s, float3 p) {
 }
 
 /* getNormal (src/rayCaster.cu:131-137). */
-template <int VTYPE, bool SLAB>
+template <int VTYPE, bool SLAB, bool SHM = false>
 __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
     /* six taps through one call site: shading runs once per hit ray, and
      * the smaller kernel keeps the traversal loop in the instruction cache */
@@ -84,7 +88,7 @@ __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
         if (t < 2) q.x = p.x + d;
         else if (t < 4) q.y = p.y + d;
         else q.z = p.z + d;
-        v[t] = interp<VTYPE, SLAB>(s, q);
+        v[t] = interp<VTYPE, SLAB, SHM>(s, q);
     }
     return normalize(f3((v[0] - v[1]) / 2.0f, (v[2] - v[3]) / 2.0f, (v[4] - v[5]) / 2.0f));
 }
@@ -102,14 +106,14 @@ __device__ __forceinline__ float3 normal_at(const Samp& s, float3 p) {
  * iso - value has the same strict sign as its own (the crossing test's
  * "no crossing" condition), so the pair keeps bracketing the crossing.
  * Each midpoint is one more trilinear sample. */
-template <int VTYPE, bool SLAB, int U>
+template <int VTYPE, bool SLAB, int U, bool SHM = false>
 __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, float tnear,
                                       int maxStep, float iso, int refine, float3* Xhit, unsigned int* nsamp) {
     float3 Xnear = add(origin, mul(ray, tnear));
     float3 Xfar = Xnear;
     float3 vStep = mul(ray, 0.5f);
     if (maxStep < 0) return false;
-    float ant = interp<VTYPE, SLAB>(s, Xnear);
+    float ant = interp<VTYPE, SLAB, SHM>(s, Xnear);
     unsigned int ns = 1;
     bool hit = false;
     for (int steps = 1; steps <= maxStep && !hit; steps += U) {
@@ -118,7 +122,7 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
 #pragma unroll
         for (int u = 0; u < U; u++) X[u] = add(u == 0 ? Xnear : X[u - 1], vStep);
 #pragma unroll
-        for (int u = 0; u < U; u++) v[u] = interp<VTYPE, SLAB>(s, X[u]);
+        for (int u = 0; u < U; u++) v[u] = interp<VTYPE, SLAB, SHM>(s, X[u]);
 #pragma unroll
         for (int u = 0; u < U; u++) {
             if (hit || steps + u > maxStep) break;
@@ -132,7 +136,7 @@ __device__ __forceinline__ bool march(const Samp& s, float3 origin, float3 ray, 
                 float3 P = Xfar, Q = X[u];
                 for (int k = 0; k < refine; k++) {
                     float3 M = mul(add(P, Q), 0.5f);
-                    float vm = interp<VTYPE, SLAB>(s, M);
+                    float vm = interp<VTYPE, SLAB, SHM>(s, M);
                     ns++;
                     if ((((iso - ant) < 0.0f) && ((iso - vm) < 0.0f)) ||
                         (((iso - ant) > 0.0f) && ((iso - vm) > 0.0f))) {
@@ -385,6 +389,23 @@ __device__ __forceinline__ bool expand(const TraceArgs& A, const RayInv& r, Stk&
     return true;
 }
 
+/* Shading of a hit at X (src/rayCaster.cu:238-250): the normal from
+ * central differences, |n . l| against the light, the colour ramp over y;
+ * the ray's hit fields for the pixel and the diagnostics. */
+template <int VTYPE, bool SLAB, bool SHM>
+__device__ __forceinline__ void shade_hit(const TraceArgs& A, Ray& R, const Samp& s, float3 X, unsigned int x,
+                                          unsigned int y, unsigned int z, unsigned int bx, unsigned int by,
+                                          unsigned int bz, unsigned int* cnt) {
+    float3 n = normal_at<VTYPE, SLAB, SHM>(s, X);
+    cnt[VT_C_NSAMPLES] += 6;
+    float3 l = normalize(sub(X, A.light));
+    float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
+    float a = X.y / 256.0f;
+    R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
+    R.hit = true; R.node = node_code(x, y, z, A.oct.Lo); R.brick = node_code(bx, by, bz, A.oct.Lc); R.n = n;
+    R.t = dot(sub(X, R.r.o), R.dir);
+}
+
 /* Candidate `ent` (a node at octreeLevel): brick lookup
  * (lruCache::updateCube, src/lruCache.cu:177-291), then march and shade
  * (src/rayCaster.cu:139-265).  CAND_MISSING when the brick is absent (it is
@@ -422,15 +443,7 @@ __device__ __forceinline__ int candidate(const TraceArgs& A, Ray& R, unsigned lo
     bool h = march<VTYPE, SLAB, U>(s, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
     cnt[VT_C_SAMPLES] += ns;
     if (!h) return CAND_EMPTY;
-    /* shade (src/rayCaster.cu:238-250) */
-    float3 n = normal_at<VTYPE, SLAB>(s, X);
-    cnt[VT_C_NSAMPLES] += 6;
-    float3 l = normalize(sub(X, A.light));
-    float dif = fabsf(n.x * l.x + n.y * l.y + n.z * l.z);
-    float a = X.y / 256.0f;
-    R.rgba = make_float4((1 - a) * dif, a * dif, 0.0f * dif, 1.0f);
-    R.hit = true; R.node = node_code(x, y, z, Lo); R.brick = node_code(bx, by, bz, Lc); R.n = n;
-    R.t = dot(sub(X, R.r.o), R.dir);
+    shade_hit<VTYPE, SLAB, false>(A, R, s, X, x, y, z, bx, by, bz, cnt);
     return CAND_HIT;
 }
 
@@ -648,7 +661,8 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
     unsigned int cnt[VT_C_COUNT];
 #pragma unroll
     for (int c = 0; c < VT_C_COUNT; c++) cnt[c] = 0;
-    const unsigned int nItems = A.ctl.in ? A.ctl.n_in : A.views.totalRays;
+    const unsigned int nItems =
+        A.ctl.in ? (A.ctl.n_in_dev ? min(*A.ctl.n_in_dev, A.ctl.n_in) : A.ctl.n_in) : A.views.totalRays;
     Stk st;
     Ray R;
     if (!PERSIST) {
@@ -694,6 +708,225 @@ __global__ void __launch_bounds__(128, 8) k_trace(TraceArgs A) {
                 else if (SKIP && s == RAY_DONE_WRITTEN) { cnt[VT_C_HITS]++; has = false; }   /* the tentative hit stands */
             }
         }
+    }
+    flush_counters(A, cnt);
+}
+
+/* ---- wavefront passes ------------------------------------------------- */
+/* Traversal round: each input ray (a fresh ray of the pass, a ray resumed
+ * from the last pass, or a ray whose candidate missed in the last round)
+ * walks its DFS (the same expansions as run_ray) to its next candidate.  An
+ * absent brick suspends the ray as in the one-kernel pass; a resident one
+ * pops the candidate, saves the ray's remaining stack as a wait record and
+ * queues a march item, counted into its slot's bin (the first item of a
+ * slot lists the slot as touched).  Where the wait pool is full the ray
+ * marches the candidate itself, as the one-kernel pass does. */
+template <int VTYPE>
+__global__ void __launch_bounds__(128, 8) k_wf_traverse(TraceArgs A, WaveRound W) {
+    __shared__ DevView sv[VT_MAX_VIEWS];
+    for (int k = threadIdx.x; k < A.views.n; k += blockDim.x) sv[k] = A.views.v[k];
+    __syncthreads();
+    unsigned int cnt[VT_C_COUNT];
+#pragma unroll
+    for (int c = 0; c < VT_C_COUNT; c++) cnt[c] = 0;
+    const unsigned int nItems =
+        A.ctl.in ? (A.ctl.n_in_dev ? min(*A.ctl.n_in_dev, A.ctl.n_in) : A.ctl.n_in) : A.views.totalRays;
+    const DevOctree& O = A.oct;
+    const int Lo = O.Lo, Lc = O.Lc, nLevels = O.nLevels, dimO = 1 << (nLevels - Lo);
+    Stk st;
+    Ray R;
+    for (unsigned int w = blockIdx.x * blockDim.x + threadIdx.x; w < nItems; w += gridDim.x * blockDim.x) {
+        const int s0 = start_ray<VTYPE, false>(A, sv, w, R, st, cnt);
+        if (s0 < 0) continue;
+        if (s0 == RAY_DONE) { write_ray(A, sv, R, cnt); continue; }
+        for (;;) {
+            bool stop = false;
+            for (;;) {   /* expand until a candidate is on top */
+                if (R.top < 0) { stop = true; break; }
+                const unsigned long long e = st.e[R.top];
+                if (e_level(e) == Lo) break;
+                R.top--;
+                cnt[VT_C_EXPANSIONS]++;
+                if (!expand(A, R.r, st, R.top, e, cnt, true)) { stop = true; break; }
+            }
+            if (stop) { write_ray(A, sv, R, cnt); break; }   /* exhausted (or stack overflow, flagged) */
+            const unsigned long long ent = st.e[R.top];
+            const unsigned int x = e_x(ent), y = e_y(ent), z = e_z(ent);
+            const unsigned int bx = x >> (Lo - Lc), by = y >> (Lo - Lc), bz = z >> (Lo - Lc);
+            const unsigned int pidx = (bx << (2 * Lc)) | (by << Lc) | bz;
+            const int slot = A.br.page[pidx];
+            if (slot < 0) {
+                if (slot == -1 || slot == VT_PAGE_SPECULATIVE) request_brick(A, pidx);
+                cnt[VT_C_DEVMISSES]++;
+                suspend_ray<VTYPE, true, false>(A, R, st, cnt);   /* the candidate stays on the stack */
+                break;
+            }
+            cnt[VT_C_CANDIDATES]++;
+            cnt[VT_C_DEVHITS]++;
+            if (slot != R.lastSlot) { A.br.stamp[slot] = A.br.pass; R.lastSlot = slot; }
+            const int mbx = (int)(x << (nLevels - Lo)), mby = (int)(y << (nLevels - Lo)), mbz = (int)(z << (nLevels - Lo));
+            float tn, tf;
+            R.top--;
+            if (!slab(R.r, mbx, mby, mbz, mbx + dimO, mby + dimO, mbz + dimO, &tn, &tf)) continue;   /* empty */
+            const unsigned int depth = (unsigned int)(R.top + 1);
+            const unsigned int q = atomicAdd(W.n_wait, 1u);
+            const unsigned long long off = atomicAdd(W.pool_wait_used, (unsigned long long)depth);
+            if (q < W.wait_cap && off + depth <= W.pool_wait_cap) {
+                for (unsigned int e = 0; e < depth; e++) W.pool_wait[off + e] = st.e[e];
+                SuspRec rec;
+                rec.ray = R.g; rec.depth = depth; rec.off = off;
+                W.wait[q] = rec;
+                const unsigned int i = atomicAdd(W.n_items, 1u);
+                if (i >= W.items_cap) { atomicOr(A.ctl.err, VT_KERR_STAGE); break; }   /* cannot happen: one item a ray */
+                const unsigned int rank = atomicAdd(&W.binCount[slot], 1u);
+                if (rank == 0) W.touched[atomicAdd(W.n_touched, 1u)] = (unsigned int)slot;
+                MarchItem it;
+                it.entry = ent; it.rec = q; it.slot = slot; it.tn = tn; it.maxStep = max_steps(tn, tf);
+                it.g = R.g; it.rank = rank; it.dx = R.dir.x; it.dy = R.dir.y; it.dz = R.dir.z; it.pad = 0;
+                W.items[i] = it;
+                break;
+            }
+            /* no room to wait: march here */
+            Samp sm;
+            int sl;
+            setup_sampler<VTYPE, true>(A, bx, by, bz, pidx, sm, &sl);
+            float3 X;
+            unsigned int ns = 0;
+            const bool h = march<VTYPE, true, 1>(sm, R.r.o, R.dir, tn, max_steps(tn, tf), A.iso, A.refine, &X, &ns);
+            cnt[VT_C_SAMPLES] += ns;
+            if (h) {
+                shade_hit<VTYPE, true, false>(A, R, sm, X, x, y, z, bx, by, bz, cnt);
+                write_ray(A, sv, R, cnt);
+                break;
+            }
+        }
+    }
+    flush_counters(A, cnt);
+}
+
+/* Bin offsets: an exclusive prefix sum of the touched slots' counts (one
+ * CTA; a few tens of thousands of slots per round). */
+__global__ void __launch_bounds__(1024) k_wf_scan(WaveRound W) {
+    __shared__ unsigned int part[1024];
+    const unsigned int nT = *W.n_touched;
+    const unsigned int per = (nT + 1023u) / 1024u;
+    const unsigned int b = threadIdx.x * per, e = min(nT, b + per);
+    unsigned int sum = 0;
+    for (unsigned int i = b; i < e; i++) sum += W.binCount[W.touched[i]];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const unsigned int v = (int)threadIdx.x >= o ? part[threadIdx.x - o] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned int base = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+    for (unsigned int i = b; i < e; i++) {
+        const unsigned int sl = W.touched[i];
+        W.binStart[sl] = base;
+        base += W.binCount[sl];
+    }
+}
+
+/* Items into slot order. */
+__global__ void k_wf_scatter(WaveRound W) {
+    const unsigned int n = min(*W.n_items, W.items_cap);
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const MarchItem it = W.items[i];
+        const unsigned int d = W.binStart[it.slot] + it.rank;
+        if (d < W.items_cap) W.sorted[d] = it;
+    }
+}
+
+/* March round: one touched slot at a time per CTA.  One thread stages the
+ * slot's brick (edge + 2 inc voxels a side, contiguous) into shared memory
+ * with a single bulk copy (cp.async.bulk, the tensor memory accelerator's
+ * non-tensor form) completing on an mbarrier; every thread then marches
+ * items of that slot from shared memory (src/rayCaster.cu:166-250, the same
+ * arithmetic as the one-kernel pass).  A hit shades and writes the pixel; a
+ * miss sends the ray's wait record on to the next traversal round, or, with
+ * nothing left on its stack, writes the background.  Waits are bounded: past
+ * the limit the CTA flags VT_KERR_STAGE and stops. */
+template <int VTYPE>
+__global__ void __launch_bounds__(128) k_wf_march(TraceArgs A, WaveRound W, unsigned int slotBytes) {
+    __shared__ DevView sv[VT_MAX_VIEWS];
+    __shared__ __align__(8) unsigned long long mbar;
+    extern __shared__ __align__(128) unsigned char wf_brick[];
+    for (int k = threadIdx.x; k < A.views.n; k += blockDim.x) sv[k] = A.views.v[k];
+    const uint32_t mb = (uint32_t)__cvta_generic_to_shared(&mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(mb), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    __syncthreads();
+    unsigned int cnt[VT_C_COUNT];
+#pragma unroll
+    for (int c = 0; c < VT_C_COUNT; c++) cnt[c] = 0;
+    const DevOctree& O = A.oct;
+    const int Lo = O.Lo, Lc = O.Lc, sh = O.nLevels - O.Lc;
+    const DevBricks& B = A.br;
+    const unsigned int nT = *W.n_touched;
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(wf_brick);
+    uint32_t phase = 0;
+    for (unsigned int t = blockIdx.x; t < nT; t += gridDim.x) {
+        const unsigned int slot = W.touched[t];
+        const unsigned int count = W.binCount[slot], start = W.binStart[slot];
+        if (threadIdx.x == 0) {
+            /* the last slot's reads (generic proxy) before this copy's writes (async proxy) */
+            asm volatile("fence.proxy.async.shared::cta;");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(mb), "r"(slotBytes) : "memory");
+            const char* src = (const char*)B.slab + (size_t)slot * slotBytes;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(dst), "l"(src), "r"(slotBytes), "r"(mb) : "memory");
+        }
+        uint32_t done = 0;
+        for (long long it = 0; it < (1ll << 22) && !done; it++) {
+            asm volatile("{\n\t.reg .pred P1;\n\t"
+                         "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                         "selp.b32 %0, 1, 0, P1;\n\t}"
+                         : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+        }
+        phase ^= 1u;
+        if (__syncthreads_or(!done)) {
+            if (threadIdx.x == 0) atomicOr(A.ctl.err, VT_KERR_STAGE);
+            break;
+        }
+        for (unsigned int k = threadIdx.x; k < count && start + k < W.items_cap; k += blockDim.x) {
+            const MarchItem it = W.sorted[start + k];
+            Ray R;
+            decode_ray(sv, A.views.n, A.tile_w, A.tile_h, it.g, R.view, R.i, R.j);
+            R.g = it.g;
+            R.dir = f3(it.dx, it.dy, it.dz);
+            R.r.o = sv[R.view].cam.pos;
+            R.hit = false;
+            const unsigned int x = e_x(it.entry), y = e_y(it.entry), z = e_z(it.entry);
+            const unsigned int bx = x >> (Lo - Lc), by = y >> (Lo - Lc), bz = z >> (Lo - Lc);
+            Samp sm;
+            sm.base = wf_brick;
+            sm.sx = (long long)B.D * B.D; sm.sy = B.D;
+            sm.ox = (int)(bx << sh) - B.inc; sm.oy = (int)(by << sh) - B.inc; sm.oz = (int)(bz << sh) - B.inc;
+            sm.hx = sm.hy = sm.hz = B.D - 2;
+            float3 X;
+            unsigned int ns = 0;
+            const bool h = march<VTYPE, true, 1, true>(sm, R.r.o, R.dir, it.tn, it.maxStep, A.iso, A.refine, &X, &ns);
+            cnt[VT_C_SAMPLES] += ns;
+            if (h) {
+                shade_hit<VTYPE, true, true>(A, R, sm, X, x, y, z, bx, by, bz, cnt);
+                write_ray(A, sv, R, cnt);
+            } else {
+                const SuspRec rec = W.wait[it.rec];
+                if (rec.depth == 0) {   /* nothing left on its stack: background */
+                    R.rgba = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+                    R.node = 0; R.brick = 0; R.t = -1.0f; R.n = f3(0, 0, 0);
+                    write_ray(A, sv, R, cnt);
+                } else {
+                    W.next[atomicAdd(W.n_next, 1u)] = rec;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) W.binCount[slot] = 0;   /* the bins start empty next round */
     }
     flush_counters(A, cnt);
 }
@@ -876,6 +1109,30 @@ cudaError_t vt_launch_trace(const TraceArgs& a, bool slabMode, bool persistent, 
     }
 #undef VT_LAUNCH_U
 #undef VT_LAUNCH
+    return cudaGetLastError();
+}
+
+cudaError_t vt_launch_wave_round(const TraceArgs& a, const WaveRound& w, int blocksPerSM, size_t slotBytes,
+                                 cudaStream_t s) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned int grid = (unsigned int)(sms * (blocksPerSM > 0 ? blocksPerSM : 8));
+    if (slotBytes % 16 != 0 || slotBytes > 200 * 1024) return cudaErrorInvalidValue;
+    static bool attr[2] = {false, false};
+    const int v = a.br.vtype == 0 ? 0 : 1;
+    if (!attr[v]) {
+        cudaError_t e = v == 0 ? cudaFuncSetAttribute(k_wf_march<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)
+                               : cudaFuncSetAttribute(k_wf_march<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr[v] = true;
+    }
+    if (v == 0) k_wf_traverse<0><<<grid, 128, 0, s>>>(a, w);
+    else k_wf_traverse<1><<<grid, 128, 0, s>>>(a, w);
+    k_wf_scan<<<1, 1024, 0, s>>>(w);
+    k_wf_scatter<<<(unsigned int)(sms * 4), 256, 0, s>>>(w);
+    if (v == 0) k_wf_march<0><<<(unsigned int)(sms * 4), 128, slotBytes, s>>>(a, w, (unsigned int)slotBytes);
+    else k_wf_march<1><<<(unsigned int)(sms * 4), 128, slotBytes, s>>>(a, w, (unsigned int)slotBytes);
     return cudaGetLastError();
 }
 

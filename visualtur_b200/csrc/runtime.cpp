@@ -184,8 +184,17 @@ struct vt_handle {
     /* timing and the pass-0 graph */
     std::vector<cudaEvent_t> ev;
     cudaGraphExec_t graph = nullptr;
+    int passKernels = 1;                   /* kernels of the last pass enqueued */
     cudaStream_t s_int = nullptr;
     std::vector<uint64_t> hint;            /* bricks to load for the next frame */
+    /* wavefront passes: per-round waiting rays (ping-pong), march items and bins */
+    struct WaveCtl { unsigned int n_wait, n_items, n_touched, n_next; unsigned long long pool_wait_used; };
+    unsigned int wave_cap = 0;
+    SuspRec* d_wwait[2] = {nullptr, nullptr}; SuspRec* d_wnext[2] = {nullptr, nullptr};
+    unsigned long long* d_wpool[2] = {nullptr, nullptr}; unsigned long long wpool_cap = 0;
+    MarchItem* d_witems = nullptr; MarchItem* d_wsorted = nullptr;
+    unsigned int* d_wbins = nullptr;    /* count, start per slot; touched list */
+    WaveCtl* d_wctl = nullptr;          /* [2] */
     /* learned prefetch on the device (vt_prefetch_predict) */
     unsigned int* d_leafPages = nullptr; int nLeaf = 0;
     float* d_feat = nullptr; float* h_feat = nullptr; float* d_probs = nullptr; int predCap = 0; int probsCap = 0;
@@ -350,6 +359,7 @@ extern "C" void vt_default_options(vt_options* o) {
     o->max_requests = 0;
     o->pool_per_ray = 0;
     o->spec_async = 1;
+    o->wavefront = 0;
 }
 
 static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
@@ -372,6 +382,7 @@ static vt_status validate(const vt_params* p, const vt_octree* o, const vt_optio
         if (opt->max_passes < 1) return fail(VT_ERR_INVALID, "max_passes must be >= 1");
         if (opt->max_suspended < 0 || opt->max_requests < 0 || opt->pool_per_ray < 0)
             return fail(VT_ERR_INVALID, "queue bounds must be >= 0 (0 = default)");
+        if (opt->wavefront < 0 || opt->wavefront > 8) return fail(VT_ERR_INVALID, "wavefront rounds must be in 0..8");
         if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
             return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
     }
@@ -466,6 +477,8 @@ extern "C" void vt_destroy(vt_handle* h) {
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     cudaFree(h->d_leafPages); cudaFree(h->d_feat); cudaFree(h->d_probs); cudaFree(h->d_pred);
+    for (int i = 0; i < 2; i++) { cudaFree(h->d_wwait[i]); cudaFree(h->d_wnext[i]); cudaFree(h->d_wpool[i]); }
+    cudaFree(h->d_witems); cudaFree(h->d_wsorted); cudaFree(h->d_wbins); cudaFree(h->d_wctl);
     if (h->h_feat) cudaFreeHost(h->h_feat);
     if (h->h_pred) cudaFreeHost(h->h_pred);
     if (h->predDone) cudaEventDestroy(h->predDone);
@@ -578,6 +591,7 @@ static vt_status collect_counters(vt_handle* h, cudaStream_t s) {
     unsigned int err = h->h_ctl->err;
     if (err & VT_KERR_STACK) return fail(VT_ERR_STACK, "a ray's traversal stack overflowed (%d entries)", VT_STACK);
     if (err & VT_KERR_NOTRESIDENT) return fail(VT_ERR_STATE, "resident render met a brick with no slot");
+    if (err & VT_KERR_STAGE) return fail(VT_ERR_TIMEOUT, "a staged brick did not arrive within its wait bound");
     if (err & VT_KERR_SUSPEND_FULL) return fail(VT_ERR_STATE, "suspended-ray list overflow (more than %u rays waiting on bricks)", h->opt.max_suspended > 0 ? std::min<unsigned int>(h->susp_cap, (unsigned int)h->opt.max_suspended) : h->susp_cap);
     return VT_OK;
 }
@@ -592,6 +606,77 @@ static vt_status ensure_events(vt_handle* h, int k) {
     return VT_OK;
 }
 
+/* wavefront passes apply: slab mode, in-order traversal, no trace log */
+static bool use_wave(const vt_handle* h, bool slabMode) {
+    return slabMode && h->opt.wavefront > 0 && h->opt.skip == 0 && !h->d_touched;
+}
+
+/* buffers of wavefront passes over up to `rays` rays */
+static vt_status ensure_wave_buffers(vt_handle* h, unsigned int rays) {
+    if (h->wave_cap >= rays && h->d_wbins) return VT_OK;
+    for (int i = 0; i < 2; i++) {
+        cudaFree(h->d_wwait[i]); cudaFree(h->d_wnext[i]); cudaFree(h->d_wpool[i]);
+        h->d_wwait[i] = h->d_wnext[i] = nullptr; h->d_wpool[i] = nullptr;
+    }
+    cudaFree(h->d_witems); cudaFree(h->d_wsorted);
+    h->d_witems = h->d_wsorted = nullptr;
+    rays = (unsigned int)std::max<unsigned long long>(rays, h->wave_cap + h->wave_cap / 2ull);
+    h->wave_cap = rays;
+    h->wpool_cap = (unsigned long long)rays * 12ull;
+    for (int i = 0; i < 2; i++) {
+        CK(cudaMalloc(&h->d_wwait[i], (size_t)rays * sizeof(SuspRec)));
+        CK(cudaMalloc(&h->d_wnext[i], (size_t)rays * sizeof(SuspRec)));
+        CK(cudaMalloc(&h->d_wpool[i], (size_t)h->wpool_cap * 8));
+    }
+    CK(cudaMalloc(&h->d_witems, (size_t)rays * sizeof(MarchItem)));
+    CK(cudaMalloc(&h->d_wsorted, (size_t)rays * sizeof(MarchItem)));
+    if (!h->d_wbins) {
+        const size_t ns = (size_t)h->cache->device_slots();
+        CK(cudaMalloc(&h->d_wbins, ns * 3 * sizeof(unsigned int)));
+        CK(cudaMemset(h->d_wbins, 0, ns * 3 * sizeof(unsigned int)));
+        CK(cudaMalloc(&h->d_wctl, 2 * sizeof(vt_handle::WaveCtl)));
+    }
+    return VT_OK;
+}
+
+/* One pass's kernels: the fused trace kernel, or wavefront rounds then the
+ * fused kernel (persistent, its ray count read on the device) for the rays
+ * still waiting.  `bound`: rays the pass can hold (wavefront buffers). */
+static cudaError_t launch_pass(vt_handle* h, const TraceArgs& a0, bool slabMode, cudaStream_t s, int* kernels) {
+    if (!use_wave(h, slabMode)) {
+        *kernels = 1;
+        return vt_launch_trace(a0, slabMode, h->opt.persistent != 0, h->opt.blocks_per_sm, s);
+    }
+    const int rounds = h->opt.wavefront;
+    const unsigned int bound = h->wave_cap;
+    const size_t ns = (size_t)h->cache->device_slots();
+    TraceArgs a = a0;
+    cudaError_t e = cudaSuccess;
+    for (int r = 0; r < rounds && e == cudaSuccess; r++) {
+        const int p = r & 1, q = p ^ 1;
+        if (r > 0) {
+            a.ctl.in = h->d_wnext[q]; a.ctl.n_in = bound; a.ctl.pool_in = h->d_wpool[q];
+            a.ctl.n_in_dev = &h->d_wctl[q].n_next;
+        }
+        WaveRound w;
+        memset(&w, 0, sizeof(w));
+        w.wait = h->d_wwait[p]; w.n_wait = &h->d_wctl[p].n_wait;
+        w.pool_wait = h->d_wpool[p]; w.pool_wait_used = &h->d_wctl[p].pool_wait_used;
+        w.pool_wait_cap = h->wpool_cap; w.wait_cap = bound;
+        w.items = h->d_witems; w.n_items = &h->d_wctl[p].n_items; w.sorted = h->d_wsorted; w.items_cap = bound;
+        w.binCount = h->d_wbins; w.binStart = h->d_wbins + ns; w.touched = h->d_wbins + 2 * ns;
+        w.n_touched = &h->d_wctl[p].n_touched;
+        w.next = h->d_wnext[p]; w.n_next = &h->d_wctl[p].n_next;
+        e = cudaMemsetAsync(&h->d_wctl[p], 0, sizeof(vt_handle::WaveCtl), s);
+        if (e == cudaSuccess) e = vt_launch_wave_round(a, w, h->opt.blocks_per_sm, h->cache->slot_bytes(), s);
+    }
+    if (e != cudaSuccess) return e;
+    const int p = (rounds - 1) & 1;
+    a.ctl.in = h->d_wnext[p]; a.ctl.n_in = bound; a.ctl.pool_in = h->d_wpool[p]; a.ctl.n_in_dev = &h->d_wctl[p].n_next;
+    *kernels = 4 * rounds + 1;
+    return vt_launch_trace(a, slabMode, true, h->opt.blocks_per_sm, s);
+}
+
 /* pass 0: clear the control block (and trace log), upload the view table,
  * launch the trace kernel -- captured once as a CUDA graph and replayed */
 static vt_status pass0(vt_handle* h, const TraceArgs& a, int nViews, bool slabMode, cudaStream_t s) {
@@ -599,7 +684,7 @@ static vt_status pass0(vt_handle* h, const TraceArgs& a, int nViews, bool slabMo
         cudaError_t e = cudaMemsetAsync(h->d_ctl, 0, sizeof(CtlBlock), q);
         if (e == cudaSuccess && h->d_touched) e = cudaMemsetAsync(h->d_touched, 0, h->touchedWords * 4, q);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_views, h->h_views, (size_t)nViews * sizeof(DevView), cudaMemcpyHostToDevice, q);
-        if (e == cudaSuccess) e = vt_launch_trace(a, slabMode, h->opt.persistent != 0, h->opt.blocks_per_sm, q);
+        if (e == cudaSuccess) e = launch_pass(h, a, slabMode, q, &h->passKernels);
         return e;
     };
     if (!h->opt.use_graph || s == 0) {
@@ -641,6 +726,8 @@ static vt_status render_views(vt_handle* h, const ViewReq* vr, int n, cudaStream
     if (st != VT_OK && h->cache && st != VT_ERR_CUDA) {
         std::string msg = vt_last_error();
         h->cache->cancel_requests(s);
+        /* wavefront bins start empty (a failed round may have left counts) */
+        if (h->d_wbins) cudaMemsetAsync(h->d_wbins, 0, (size_t)h->cache->device_slots() * 4, s);
         fail(st, "%s", msg.c_str());
     }
     return st;
@@ -676,9 +763,11 @@ static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cuda
     if (slabMode) { h->cache->begin_frame(); a.br.pass = h->cache->next_pass(); }
     if ((st = ensure_events(h, 0)) != VT_OK) return st;
     CK(cudaEventRecord(h->ev[0], s));
+    if (use_wave(h, slabMode) && (st = ensure_wave_buffers(h, std::max<unsigned int>((unsigned int)base, h->susp_cap))) != VT_OK)
+        return st;
     if ((st = pass0(h, a, n, slabMode, s)) != VT_OK) return st;
     CK(cudaEventRecord(h->ev[1], s));
-    h->stats.launches++;
+    h->stats.launches += h->passKernels;
     int passes = 1;
     double stall = 0, h2d = 0, wait = 0;
     /* prefetch hint for the next frame: host-tier loads overlap this frame's kernel */
@@ -735,9 +824,10 @@ static vt_status render_views_inner(vt_handle* h, const ViewReq* vr, int n, cuda
             CK(cudaMemsetAsync(&h->d_ctl->n_out, 0, offsetof(CtlBlock, pool_used) + 8 - offsetof(CtlBlock, n_out), s));
             if ((st = ensure_events(h, passes)) != VT_OK) return st;
             CK(cudaEventRecord(h->ev[2 * passes], s));
-            CK(vt_launch_trace(a, slabMode, h->opt.persistent != 0, h->opt.blocks_per_sm, s));
+            int nk = 1;
+            CK(launch_pass(h, a, slabMode, s, &nk));
             CK(cudaEventRecord(h->ev[2 * passes + 1], s));
-            h->stats.launches++;
+            h->stats.launches += nk;
             passes++;
             if ((st = h->cache->spec_work(h->ev[2 * passes - 1], nullptr)) != VT_OK) return st;
         }
@@ -854,6 +944,7 @@ extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
     o.pops = t->pops; o.blocks_per_sm = t->blocks_per_sm; o.lookahead = t->lookahead; o.use_graph = t->use_graph;
     o.skip = t->skip;
     o.spec_async = t->spec_async;
+    o.wavefront = t->wavefront;
     vt_status s = validate(&h->p, h->oct, &o);
     if (s != VT_OK) return s;
     if (o.lookahead < 0 || o.lookahead > 64 || o.pops < 1 || o.blocks_per_sm < 1 || o.blocks_per_sm > 32)
@@ -871,6 +962,7 @@ extern "C" vt_status vt_get_tuning(vt_handle* h, vt_tuning* t) {
     t->use_graph = h->opt.use_graph;
     t->skip = h->opt.skip;
     t->spec_async = h->opt.spec_async;
+    t->wavefront = h->opt.wavefront;
     return VT_OK;
 }
 

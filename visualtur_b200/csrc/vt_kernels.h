@@ -14,6 +14,7 @@
 #define VT_KERR_STACK 1u        /* a ray's stack overflowed */
 #define VT_KERR_NOTRESIDENT 2u  /* resident mode met a brick with no slot */
 #define VT_KERR_SUSPEND_FULL 4u /* suspended-ray list overflowed */
+#define VT_KERR_STAGE 8u        /* a bounded wait for a staged brick gave up */
 /* page-table states besides a slot index: -1 absent, and */
 #define VT_PAGE_REQUESTED (-2)     /* a ray waits on the brick */
 #define VT_PAGE_SPECULATIVE (-3)   /* requested ahead of need (lookahead) */
@@ -101,6 +102,7 @@ struct DevCtl {
     unsigned int* err;
     unsigned int* work;                         /* persistent-kernel work counter */
     const SuspRec* in; unsigned int n_in;      /* rays to resume (NULL: pass 0) */
+    const unsigned int* n_in_dev;               /* if set: the count, in device memory (n_in bounds it) */
     const unsigned long long* pool_in;
     SuspRec* out; unsigned int* n_out; unsigned int out_cap;
     unsigned long long* pool_out; unsigned long long* pool_used; unsigned long long pool_cap;
@@ -125,8 +127,43 @@ struct TraceArgs {
     int refine;                                 /* bisection steps before the linear refinement */
 };
 
+/* Wavefront passes (slab mode): a traversal kernel walks each ray's DFS to
+ * its next candidate whose brick is resident and queues (ray, candidate)
+ * as a march item, binned by brick slot; a march kernel stages each binned
+ * slot into shared memory with one bulk copy and marches its items from
+ * there.  Rays whose candidate missed wait (their stack in a wait pool) for
+ * the next traversal round. */
+struct MarchItem {
+    unsigned long long entry;   /* the candidate's stack entry */
+    unsigned int rec;           /* the ray's wait record (its remaining stack) */
+    int slot;                   /* brick slot */
+    float tn;                   /* candidate slab entry parameter */
+    int maxStep;                /* march steps */
+    unsigned int g;             /* padded global ray index */
+    unsigned int rank;          /* position among the slot's items */
+    float dx, dy, dz;           /* ray direction */
+    unsigned int pad;
+};
+struct WaveRound {
+    /* input of this round: the pass's rays (in == NULL in a first pass: ray
+     * indices 0..count) or the previous round's waiting records */
+    const SuspRec* in; const unsigned int* n_in; unsigned int n_in_host; const unsigned long long* pool_in;
+    /* waiting rays of this round */
+    SuspRec* wait; unsigned int* n_wait; unsigned long long* pool_wait; unsigned long long* pool_wait_used;
+    unsigned long long pool_wait_cap; unsigned int wait_cap;
+    /* march items, binned by slot */
+    MarchItem* items; unsigned int* n_items; MarchItem* sorted; unsigned int items_cap;
+    unsigned int* binCount; unsigned int* binStart; unsigned int* touched; unsigned int* n_touched;
+    /* rays whose candidate missed: the next round's input */
+    SuspRec* next; unsigned int* n_next;
+    unsigned int* work;         /* persistent work counter */
+    int last;                   /* last round: misses join the pass's suspended list instead */
+};
+
 /* launchers (render.cu) */
 cudaError_t vt_launch_trace(const TraceArgs& a, bool slab, bool persistent, int blocks_per_sm, cudaStream_t s);
+cudaError_t vt_launch_wave_round(const TraceArgs& a, const WaveRound& w, int blocks_per_sm, size_t slotBytes,
+                                 cudaStream_t s);
 cudaError_t vt_launch_rays(const DevCamera& c, float* dirs, cudaStream_t s);
 cudaError_t vt_launch_cube(const DevCamera& c, const float* cube, int3 minBox, int3 cubeDim,
                            int3 cubeInc, float iso, float3 light, float4* rgba, cudaStream_t s);
