@@ -924,13 +924,13 @@ def run_ours(args, cfg, rank, world, torch, dist):
     if args.skip is not None:
         wl.r.set_tuning(skip=args.skip)
     if not cfg["resident"]:
-        wl.r.set_tuning(spec_async=args.spec_async)
+        wl.r.set_tuning(spec_async=args.spec_async, wavefront=args.wavefront)
     if M["autotune"] and not args.no_autotune:
         tune = autotune(args, wl, cfg, torch, dev, stream, frame0, batch)
         if args.skip is not None:      # the brick sweep may have built a new renderer
             wl.r.set_tuning(skip=args.skip)
         if not cfg["resident"]:
-            wl.r.set_tuning(spec_async=args.spec_async)
+            wl.r.set_tuning(spec_async=args.spec_async, wavefront=args.wavefront)
     if P is not None:
         P.set_bricks(wl.r.brick_list(), wl.oc.nLevels - int(round(math.log2(wl.brick))))
     L = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch, predictor=P, warm=args.warm)
@@ -1019,7 +1019,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
         conf = {"views_per_launch": cfg["views"]["n"], "resolutions": [list(r) for r in cfg["views"]["res"]],
                 "rays_per_step": round(rays_rank / args.steps), "skip": skip_used}
     else:
-        conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": skip_used}
+        conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": skip_used,
+                "wavefront": wl.r.tuning()["wavefront"]}
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
@@ -1179,6 +1180,8 @@ def main():
     ap.add_argument("--paging", default=None, help="fly-throughs: fixed FRAMES,LOOKAHEAD[,HINT_THRESHOLD[,SKIP]] "
                                                    "instead of the paging autotune")
     ap.add_argument("--warm", action="store_true", help="profiling: preloaded cache, no cold start")
+    ap.add_argument("--wavefront", type=int, default=0,
+                    help="wavefront rounds per pass (0: the fused trace kernel; slab mode, in-order traversal)")
     ap.add_argument("--spec-async", type=int, default=1, choices=(0, 1),
                     help="1: lookahead bricks load on the cache's side stream while passes run; 0: with the demand "
                          "requests of the same service")
