@@ -937,6 +937,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     if paging and P is not None:
         L.thr = paging["best"]["hint_threshold"]
     skip_used = wl.r.tuning()["skip"]
+    wave_used = wl.r.tuning()["wavefront"]
     e2e_raw = {}
     ms, per, launches, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index),
                                           cfg["l2flush"], e2e=e2e_raw)
@@ -1020,7 +1021,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
                 "rays_per_step": round(rays_rank / args.steps), "skip": skip_used}
     else:
         conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": skip_used,
-                "wavefront": wl.r.tuning()["wavefront"]}
+                "wavefront": wave_used}
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
