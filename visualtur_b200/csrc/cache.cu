@@ -360,10 +360,14 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
     }
     CKC(cudaMemcpyAsync(h_req_, d_req, (size_t)nReq * 8, cudaMemcpyDeviceToHost, s));
     /* the pass's slot stamps come with the request list, so victim choice
-     * never waits for a fill in flight */
-    if (!stampsFresh_) CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
+     * never waits for a fill in flight -- unless never-filled slots can take
+     * every request (a cold start), when no victim is chosen and speculative
+     * requests only join the side stream's queue */
+    const bool needStamps = !(asyncSpec_ && (size_t)nReq <= freeSlots_.size());
+    if (!stampsFresh_ && needStamps)
+        CKC(cudaMemcpyAsync(stampHost_.data(), d_stamp_, (size_t)nSlots_ * 4, cudaMemcpyDeviceToHost, s));
     CKC(cudaStreamSynchronize(s));
-    stampsFresh_ = true;
+    if (needStamps) stampsFresh_ = true;
     requested_ += nReq;
     std::vector<uint64_t> demand, spec;
     demand.reserve(nReq);

@@ -290,12 +290,9 @@ template <class TA, class TB>
 static cudaError_t gemm(bool tc, const TA* A, long long am, long long ak, const TB* B, long long bk, long long bn,
                         float* C, long long cm, int M, int N, int K, const float* bias, int act, int acc, cudaStream_t s) {
     if (tc) {
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-            if (e != cudaSuccess) return e;
-            attr = true;
-        }
+        /* per launch (a cheap host call): the attribute belongs to the current device */
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+        if (e != cudaSuccess) return e;
         dim3 grid((N + TC_N - 1) / TC_N, (M + TC_M - 1) / TC_M);
         k_gemm_tc<TA, TB><<<grid, 128, TC_SMEM, s>>>(A, am, ak, B, bk, bn, C, cm, M, N, K, bias, act, acc);
         return cudaGetLastError();

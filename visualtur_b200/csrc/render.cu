@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(128, 8) k_wf_traverse(TraceArgs A, WaveRound W
                 rec.ray = R.g; rec.depth = depth; rec.off = off;
                 W.wait[q] = rec;
                 const unsigned int i = atomicAdd(W.n_items, 1u);
-                if (i >= W.items_cap) { atomicOr(A.ctl.err, VT_KERR_STAGE); break; }   /* cannot happen: one item a ray */
+                if (i >= W.items_cap) { atomicOr(A.ctl.err, VT_KERR_WAVE); break; }   /* cannot happen: one item a ray */
                 const unsigned int rank = atomicAdd(&W.binCount[slot], 1u);
                 if (rank == 0) W.touched[atomicAdd(W.n_touched, 1u)] = (unsigned int)slot;
                 MarchItem it;
@@ -1119,14 +1119,11 @@ cudaError_t vt_launch_wave_round(const TraceArgs& a, const WaveRound& w, int blo
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const unsigned int grid = (unsigned int)(sms * (blocksPerSM > 0 ? blocksPerSM : 8));
     if (slotBytes % 16 != 0 || slotBytes > 200 * 1024) return cudaErrorInvalidValue;
-    static bool attr[2] = {false, false};
+    /* per launch (a cheap host call): the attribute belongs to the current device */
     const int v = a.br.vtype == 0 ? 0 : 1;
-    if (!attr[v]) {
-        cudaError_t e = v == 0 ? cudaFuncSetAttribute(k_wf_march<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)
-                               : cudaFuncSetAttribute(k_wf_march<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) return e;
-        attr[v] = true;
-    }
+    cudaError_t e = v == 0 ? cudaFuncSetAttribute(k_wf_march<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)
+                           : cudaFuncSetAttribute(k_wf_march<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e != cudaSuccess) return e;
     if (v == 0) k_wf_traverse<0><<<grid, 128, 0, s>>>(a, w);
     else k_wf_traverse<1><<<grid, 128, 0, s>>>(a, w);
     k_wf_scan<<<1, 1024, 0, s>>>(w);

@@ -592,6 +592,7 @@ static vt_status collect_counters(vt_handle* h, cudaStream_t s) {
     if (err & VT_KERR_STACK) return fail(VT_ERR_STACK, "a ray's traversal stack overflowed (%d entries)", VT_STACK);
     if (err & VT_KERR_NOTRESIDENT) return fail(VT_ERR_STATE, "resident render met a brick with no slot");
     if (err & VT_KERR_STAGE) return fail(VT_ERR_TIMEOUT, "a staged brick did not arrive within its wait bound");
+    if (err & VT_KERR_WAVE) return fail(VT_ERR_STATE, "a wavefront round ran out of march-item room");
     if (err & VT_KERR_SUSPEND_FULL) return fail(VT_ERR_STATE, "suspended-ray list overflow (more than %u rays waiting on bricks)", h->opt.max_suspended > 0 ? std::min<unsigned int>(h->susp_cap, (unsigned int)h->opt.max_suspended) : h->susp_cap);
     return VT_OK;
 }

@@ -15,6 +15,7 @@
 #define VT_KERR_NOTRESIDENT 2u  /* resident mode met a brick with no slot */
 #define VT_KERR_SUSPEND_FULL 4u /* suspended-ray list overflowed */
 #define VT_KERR_STAGE 8u        /* a bounded wait for a staged brick gave up */
+#define VT_KERR_WAVE 16u        /* a wavefront round ran out of item room (cannot happen: one item a ray) */
 /* page-table states besides a slot index: -1 absent, and */
 #define VT_PAGE_REQUESTED (-2)     /* a ray waits on the brick */
 #define VT_PAGE_SPECULATIVE (-3)   /* requested ahead of need (lookahead) */
