@@ -119,6 +119,10 @@ MODES = {
 }
 
 
+# demand loads copy x/y aprons from resident neighbours (both renderers)
+SHARED_APRONS = 1
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -398,7 +402,8 @@ class Workload:
         """A renderer in `mode` (cold cache unless the workload is resident
         or `warm`: every needed brick preloaded, for steady-state profiles)."""
         opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=0,
-                                      preload=1 if (self.cfg["resident"] or warm) else 0, **MODES[mode]["opts"])
+                                      preload=1 if (self.cfg["resident"] or warm) else 0,
+                                      shared_aprons=SHARED_APRONS, **MODES[mode]["opts"])
         return self.vt.visualTur(self.params(brick), opt, volume=self.fm, octree=self.oc)
 
     def train_prefetcher(self, torch, poses=20000, paths=100, W=240, H=135, epochs=30):
@@ -1022,6 +1027,8 @@ def run_ours(args, cfg, rank, world, torch, dist):
     else:
         conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": skip_used,
                 "wavefront": wave_used}
+    if not cfg["resident"]:
+        conf["shared_aprons"] = SHARED_APRONS
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
@@ -1053,6 +1060,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
                         "first_launch_stall_ms": round(per[0]["ms_stall_last_frame"], 3),
                         "host_read_ms_total": round(st["ms_host_read_total"], 2),
                         "fill_wait_ms_total": round(st["ms_fill_wait_total"], 2),
+                        "h2d_gb_total": round(sum(s["bytes_h2d_last_frame"] for s in per) / 1e9, 4),
                         "hits": st["hits"], "samples": st["samples"], "candidates": st["candidates"],
                         "expansions": st["expansions"]},
     }
@@ -1189,7 +1197,11 @@ def main():
     ap.add_argument("--skip", type=int, default=None,
                     help="absent-brick candidates a ray may set aside per pass (default: tuned on fly-throughs, 0 on "
                          "batched views)")
+    ap.add_argument("--shared-aprons", type=int, default=1, choices=(0, 1),
+                    help="1: demand loads copy x/y aprons from resident neighbours' slots; 0: whole bricks")
     args = ap.parse_args()
+    global SHARED_APRONS
+    SHARED_APRONS = args.shared_aprons
     if args.warmup < 3:
         args.warmup = 3
     import torch

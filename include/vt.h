@@ -225,6 +225,11 @@ typedef struct {
      * rays still waiting.  Same image.  Slab mode, in-order traversal
      * (skip 0) only. */
     int wavefront;
+    /* 1: a demand load copies a brick's x and y aprons from the slots of
+     * resident neighbours (whose middles hold the same voxels) and reads
+     * and transfers only the rest; 0: every load reads and transfers the
+     * whole brick.  Same bricks either way. */
+    int shared_aprons;
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -254,9 +259,10 @@ vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], i
  * march unroll, persistent ray queue, traversal steps between refills,
  * persistent CTAs per SM, lookahead requests, graph replay, absent-brick
  * candidates set aside per pass, side-stream lookahead loads, wavefront
- * rounds. */
+ * rounds, shared aprons. */
 typedef struct {
-    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip, spec_async, wavefront;
+    int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip, spec_async, wavefront,
+        shared_aprons;
 } vt_tuning;
 vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t);
 vt_status vt_get_tuning(vt_handle* h, vt_tuning* t);

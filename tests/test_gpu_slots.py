@@ -1,8 +1,9 @@
 """A device slot must hold exactly the zero-padded box
 [min - inc, min + edge + inc) of the volume (lruCache's brick,
-src/lruCache.cu:224-226), whichever way the service filled it (copy-engine
-runs of consecutive slots, the fill kernel, slots reused within a
-service).  Checked slot by slot against the volume (vt_debug_slot) and
+src/lruCache.cu:224-226), whichever way the service filled it (whole
+bricks or some parts from the packed host tier, x/y aprons copied from
+neighbouring slots, slots reused within a service, lookahead bricks on the
+side stream or with the demand ones).  Checked slot by slot against the volume (vt_debug_slot) and
 frame by frame against the resident renderer, for float32 and uint8
 voxels, a non-cubic volume (bricks on its faces and beyond it), an apron
 wider than the brick, and device caches small enough that slots are reused
@@ -52,13 +53,16 @@ def decode(code, Lc):
     return c
 
 
-@pytest.mark.parametrize("dtype,levelC,inc,dev", [
-    (np.float32, 4, 3, 4096),     # every brick fits: long copy-engine runs
-    (np.float32, 4, 3, 60),       # slots reused within a frame's services
-    (np.uint8, 4, 4, 90),         # byte voxels, wider apron
-    (np.float32, 5, 5, 300),      # apron wider than the brick (inc 5 > edge 4)
+@pytest.mark.parametrize("dtype,levelC,inc,dev,opts", [
+    (np.float32, 4, 3, 4096, {}),     # every brick fits
+    (np.float32, 4, 3, 60, {}),       # slots reused within a frame's services
+    (np.uint8, 4, 4, 90, {}),         # byte voxels, wider apron
+    (np.float32, 5, 5, 300, {}),      # apron wider than the brick (inc 5 > edge 4)
+    (np.float32, 4, 3, 60, {"shared_aprons": 0}),                  # whole bricks only
+    (np.uint8, 4, 3, 4096, {"spec_async": 0}),                     # lookahead with the demand loads
+    (np.float32, 3, 3, 200, {"spec_async": 0, "lookahead": 0}),    # 16^3 bricks, demand loads only
 ])
-def test_slots_hold_the_padded_box(dtype, levelC, inc, dev, tmp_path, cuda):
+def test_slots_hold_the_padded_box(dtype, levelC, inc, dev, opts, tmp_path, cuda):
     vol, iso = volume(dtype)
     fm = vt.FileManager.wrap(vol)
     path = os.path.join(str(tmp_path), "vol.oct")
@@ -71,8 +75,10 @@ def test_slots_hold_the_padded_box(dtype, levelC, inc, dev, tmp_path, cuda):
         p = vt.make_params(W=W, H=H, octreeFile=None, hdf5File=None, octreeLevel=levelC + 1, levelCubes=levelC,
                            dimCube=edge, cubeInc=inc, distance=50.0, fov_H=30.0, fov_W=30.0,
                            maxElementsCache=nslots, maxElementsCache_CPU=max(nslots, 64))
-        return vt.visualTur(p, vt.default_options(resident=resident, record_hits=0, preload=0, lookahead=2,
-                                                  max_passes=4096), volume=fm, octree=oc)
+        o = dict(resident=resident, record_hits=0, preload=0, lookahead=2, max_passes=4096)
+        if not resident:
+            o.update(opts)
+        return vt.visualTur(p, vt.default_options(**o), volume=fm, octree=oc)
 
     ref = make(1, 8)
     dem = make(0, dev)

@@ -29,15 +29,104 @@ namespace vtrt {
         if (e_ != cudaSuccess) return fail(VT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
-/* one CTA per brick: 16-byte copies from mapped host memory */
-__global__ void k_fill_bricks(const unsigned char* __restrict__ tier, size_t slotBytes, const int2* __restrict__ pairs,
-                              unsigned char* __restrict__ slab) {
-    int2 p = pairs[blockIdx.x];
-    const uint4* src = (const uint4*)(tier + (size_t)p.x * slotBytes);
-    uint4* dst = (uint4*)(slab + (size_t)p.y * slotBytes);
-    size_t n = slotBytes / 16;
-    for (size_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+/* Warp-cooperative copy of n bytes: 16-byte words where source and
+ * destination agree modulo 16, else 4-byte words where they agree modulo
+ * 4, else bytes; four words in flight per lane (loads from mapped host
+ * memory cross PCIe). */
+template <typename W>
+__device__ __forceinline__ void warp_copy_w(unsigned char* d, const unsigned char* q, size_t n, int lane) {
+    const size_t a = sizeof(W);
+    size_t head = (a - ((size_t)d & (a - 1))) & (a - 1);
+    if (head > n) head = n;
+    if ((size_t)lane < head) d[lane] = q[lane];
+    d += head; q += head; n -= head;
+    const size_t nw = n / a;
+    W* dw = (W*)d;
+    const W* qw = (const W*)q;
+    for (size_t i = lane; i < nw; i += 128) {
+        W v0 = qw[i], v1, v2, v3;
+        if (i + 32 < nw) v1 = qw[i + 32];
+        if (i + 64 < nw) v2 = qw[i + 64];
+        if (i + 96 < nw) v3 = qw[i + 96];
+        dw[i] = v0;
+        if (i + 32 < nw) dw[i + 32] = v1;
+        if (i + 64 < nw) dw[i + 64] = v2;
+        if (i + 96 < nw) dw[i + 96] = v3;
+    }
+    const size_t t = nw * a;
+    if ((size_t)lane < n - t) d[t + lane] = q[t + lane];
 }
+__device__ __forceinline__ void warp_copy(unsigned char* d, const unsigned char* q, size_t n, int lane) {
+    const size_t x = (size_t)d ^ (size_t)q;
+    if ((x & 15) == 0) warp_copy_w<uint4>(d, q, n, lane);
+    else if ((x & 3) == 0) warp_copy_w<unsigned int>(d, q, n, lane);
+    else warp_copy_w<unsigned char>(d, q, n, lane);
+}
+
+/* Brick loads, one CTA per brick, in up to three launches on one stream:
+ * phase 1 copies the parts the brick takes from the host tier (mapped
+ * memory, packed by part) into its slot; phase 2 the y aprons from the y
+ * neighbours' middles; phase 3 the x aprons from the x neighbours' planes,
+ * which by then hold their own y aprons. */
+__global__ void k_fill_split(const unsigned char* __restrict__ tier, const unsigned char* __restrict__ stage,
+                             unsigned char* __restrict__ slab, TierGeo g, const SplitItem* __restrict__ items,
+                             int phase) {
+    const SplitItem it = items[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int e = g.e, inc = g.inc;
+    unsigned char* dst = slab + (size_t)it.slot * g.slotBytes;
+    const size_t row = (size_t)g.D * g.es, plane = (size_t)g.D * row;
+    if (phase == 1) {
+        const unsigned char* src = (it.staged ? stage : tier) + (size_t)it.hs * g.tierBytes;
+        /* one chunk per plane of a part: [0, e) M, then inc X- planes, inc
+         * X+ planes, e Y- and e Y+ plane pieces */
+        for (int c = warp; c < 3 * e + 2 * inc; c += nwarps) {
+            int b, q;
+            size_t soff, doff, len;
+            if (c < e) {
+                b = 0; q = c;
+                soff = g.off[0] + (size_t)q * e * row; doff = (size_t)(inc + q) * plane + (size_t)inc * row;
+                len = (size_t)e * row;
+            } else if (c < e + 2 * inc) {
+                const bool lo = c < e + inc;
+                b = lo ? 1 : 2; q = lo ? c - e : c - e - inc;
+                soff = g.off[b] + (size_t)q * plane; doff = (size_t)(lo ? q : inc + e + q) * plane; len = plane;
+            } else {
+                const bool lo = c < 2 * e + 2 * inc;
+                b = lo ? 3 : 4; q = lo ? c - e - 2 * inc : c - 2 * e - 2 * inc;
+                soff = g.off[b] + (size_t)q * inc * row;
+                doff = (size_t)(inc + q) * plane + (lo ? 0 : (size_t)(inc + e) * row);
+                len = (size_t)inc * row;
+            }
+            if (it.parts & (1 << b)) warp_copy(dst + doff, src + soff, len, lane);
+        }
+    } else if (phase == 2) {
+        /* Y-: rows [0, inc) = the (y-1) neighbour's rows [e, e+inc); Y+: rows
+         * [inc+e, D) = the (y+1) neighbour's rows [inc, 2 inc) */
+        for (int c = warp; c < 2 * e; c += nwarps) {
+            const bool lo = c < e;
+            const int nb = it.nb[lo ? 2 : 3];
+            if (nb < 0) continue;
+            const int p = lo ? c : c - e;
+            const size_t doff = (size_t)(inc + p) * plane + (lo ? 0 : (size_t)(inc + e) * row);
+            const size_t soff = lo ? doff + (size_t)e * row : doff - (size_t)e * row;
+            warp_copy(dst + doff, slab + (size_t)nb * g.slotBytes + soff, (size_t)inc * row, lane);
+        }
+    } else {
+        /* X-: planes [0, inc) = the (x-1) neighbour's planes [e, e+inc); X+:
+         * planes [inc+e, D) = the (x+1) neighbour's planes [inc, 2 inc) */
+        for (int c = warp; c < 2 * inc; c += nwarps) {
+            const bool lo = c < inc;
+            const int nb = it.nb[lo ? 0 : 1];
+            if (nb < 0) continue;
+            const int q = lo ? c : c - inc;
+            const size_t doff = (size_t)(lo ? q : inc + e + q) * plane;
+            const size_t soff = (size_t)(lo ? e + q : inc + q) * plane;
+            warp_copy(dst + doff, slab + (size_t)nb * g.slotBytes + soff, plane, lane);
+        }
+    }
+}
+
 /* page-table / stamp updates: x = page index, y = value; slot stamps for
  * loaded bricks */
 __global__ void k_page_update(int* page, const int2* upd, int n, unsigned int* stamp, unsigned int stampValue) {
@@ -58,19 +147,22 @@ BrickCache::~BrickCache() {
     if (specStream_) cudaStreamSynchronize(specStream_);
     for (SpecChunk& C : chunks_) {
         if (C.ev) cudaEventDestroy(C.ev);
-        if (C.hp) cudaFreeHost(C.hp);
+        if (C.hi) cudaFreeHost(C.hi);
         if (C.hu) cudaFreeHost(C.hu);
-        cudaFree(C.dp); cudaFree(C.du);
+        cudaFree(C.di); cudaFree(C.du);
     }
     if (specStream_) cudaStreamDestroy(specStream_);
-    cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_);
+    cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_); cudaFree(d_stage_);
     if (h_tier_) cudaFreeHost(h_tier_);
     for (Xfer& X : xf_) {
         if (X.ev) cudaEventSynchronize(X.ev), cudaEventDestroy(X.ev);
-        if (X.hp) cudaFreeHost(X.hp);
         if (X.hu) cudaFreeHost(X.hu);
-        cudaFree(X.dp); cudaFree(X.du);
+        if (X.hi) cudaFreeHost(X.hi);
+        cudaFree(X.du); cudaFree(X.di);
     }
+    if (svcItemsH_) cudaFreeHost(svcItemsH_);
+    if (svcUpdH_) cudaFreeHost(svcUpdH_);
+    cudaFree(svcItemsD_); cudaFree(svcUpdD_);
     if (h_req_) cudaFreeHost(h_req_);
 
 }
@@ -83,6 +175,50 @@ vt_status BrickCache::init(const CacheConfig& c) {
     D_ = c.edge + 2 * c.inc;
     slotBytes_ = ((size_t)D_ * D_ * D_ * esize_ + 15) & ~(size_t)15;
     brickVol_ = slotBytes_ / esize_;
+    {
+        TierGeo& g = geo_;
+        g.D = D_; g.e = c.edge; g.inc = c.inc; g.es = esize_;
+        const size_t row = (size_t)D_ * esize_;
+        g.len[0] = (size_t)c.edge * c.edge * row;                        /* M */
+        g.len[1] = g.len[2] = (size_t)c.inc * D_ * row;                  /* X-, X+ */
+        g.len[3] = g.len[4] = (size_t)c.edge * c.inc * row;              /* Y-, Y+ */
+        size_t o = 0;
+        for (int b = 0; b < 5; b++) { g.off[b] = o; o = (o + g.len[b] + 63) & ~(size_t)63; }
+        g.tierBytes = tierBytes_ = o;
+        g.slotBytes = slotBytes_;
+        /* rows of every part mask, in the volume's (plane, row) order, with
+         * their packed offsets */
+        if (tierBytes_ > 0xFFFFFFFFull) return fail(VT_ERR_INVALID, "brick too large");
+        const int D = D_, e = c.edge, inc = c.inc;
+        for (int parts = 0; parts < 32; parts++) {
+            std::vector<TierRow>& L = rowList_[parts];
+            L.clear();
+            for (int x = 0; x < D; x++) {
+                if (x < inc || x >= inc + e) {
+                    const bool lo = x < inc;
+                    if (!(parts & (lo ? kPartXm : kPartXp))) continue;
+                    const size_t base = g.off[lo ? 1 : 2] + (size_t)(lo ? x : x - inc - e) * D * row;
+                    for (int y = 0; y < D; y++) L.push_back({x, y, (unsigned int)(base + (size_t)y * row)});
+                    continue;
+                }
+                const int p = x - inc;
+                for (int y = 0; y < D; y++) {
+                    size_t o2;
+                    if (y < inc) {
+                        if (!(parts & kPartYm)) continue;
+                        o2 = g.off[3] + ((size_t)p * inc + y) * row;
+                    } else if (y >= inc + e) {
+                        if (!(parts & kPartYp)) continue;
+                        o2 = g.off[4] + ((size_t)p * inc + (y - inc - e)) * row;
+                    } else {
+                        if (!(parts & kPartM)) continue;
+                        o2 = g.off[0] + ((size_t)p * e + (y - inc)) * row;
+                    }
+                    L.push_back({x, y, (unsigned int)o2});
+                }
+            }
+        }
+    }
     pageBase_ = 0;                     /* keys are page indices (bx << 2Lc | by << Lc | bz) */
     pageN_ = (size_t)1 << (3 * c.Lc);
     nSlots_ = c.deviceSlots;
@@ -90,9 +226,11 @@ vt_status BrickCache::init(const CacheConfig& c) {
     CKC(cudaMalloc(&d_page_, pageN_ * 4));
     CKC(cudaMemset(d_page_, 0xFF, pageN_ * 4));
     CKC(cudaMalloc(&d_slab_, slotBytes_ * (size_t)nSlots_));
+    stageCap_ = std::min<size_t>(4096, (size_t)nSlots_);
+    CKC(cudaMalloc(&d_stage_, stageCap_ * tierBytes_));
     CKC(cudaMalloc(&d_stamp_, (size_t)nSlots_ * 4));
     CKC(cudaMemset(d_stamp_, 0, (size_t)nSlots_ * 4));
-    CKC(cudaHostAlloc((void**)&h_tier_, slotBytes_ * (size_t)nHost_, cudaHostAllocMapped | cudaHostAllocPortable));
+    CKC(cudaHostAlloc((void**)&h_tier_, tierBytes_ * (size_t)nHost_, cudaHostAllocMapped | cudaHostAllocPortable));
     CKC(cudaHostGetDevicePointer(&d_tier_, h_tier_, 0));
     slotBrick_.assign(nSlots_, kEmpty);
     mark_.assign(nSlots_, 0);
@@ -105,6 +243,8 @@ vt_status BrickCache::init(const CacheConfig& c) {
     freeHost_.resize(nHost_);
     for (int i = 0; i < nHost_; i++) freeHost_[i] = nHost_ - 1 - i;
     hostTick_.assign(nHost_, 0);
+    hostMask_.assign(nHost_, 0);
+    sharedAprons_ = c.sharedAprons;
     slotBusy_.assign(nSlots_, 0);
     hostBusy_.assign(nHost_, 0);
     asyncSpec_ = c.asyncSpec;
@@ -117,9 +257,9 @@ vt_status BrickCache::init(const CacheConfig& c) {
             SpecChunk& C = chunks_[i];
             C.cap = kSpecChunk;
             CKC(cudaEventCreateWithFlags(&C.ev, cudaEventDisableTiming));
-            CKC(cudaHostAlloc((void**)&C.hp, C.cap * sizeof(int2), cudaHostAllocDefault));
+            CKC(cudaHostAlloc((void**)&C.hi, C.cap * sizeof(SplitItem), cudaHostAllocDefault));
             CKC(cudaHostAlloc((void**)&C.hu, C.cap * sizeof(int2), cudaHostAllocDefault));
-            CKC(cudaMalloc(&C.dp, C.cap * sizeof(int2)));
+            CKC(cudaMalloc(&C.di, C.cap * sizeof(SplitItem)));
             CKC(cudaMalloc(&C.du, C.cap * sizeof(int2)));
             chunkFree_.push_back(kSpecChunks - 1 - i);
         }
@@ -132,29 +272,97 @@ void BrickCache::fill_args(DevBricks& b) const {
     b.inc = cfg_.inc; b.vtype = cfg_.vol->vtype; b.stamp = d_stamp_; b.pass = pass_;
 }
 
-bool BrickCache::read_brick(uint64_t page, void* dst) const {
-    const int Lc = cfg_.Lc, sh = cfg_.nLevels - cfg_.Lc;
+double BrickCache::part_bytes(int parts) const {
+    double n = 0;
+    for (int b = 0; b < 5; b++)
+        if (parts & (1 << b)) n += (double)geo_.len[b];
+    return n;
+}
+
+bool BrickCache::read_part(uint64_t page, int part, unsigned char* img) const {
+    const int Lc = cfg_.Lc, sh = cfg_.nLevels - cfg_.Lc, inc = cfg_.inc, e = cfg_.edge, D = D_;
     const uint64_t msk = (1ull << Lc) - 1;
-    int3 m = make_int3((int)((page >> (2 * Lc)) << sh), (int)(((page >> Lc) & msk) << sh), (int)((page & msk) << sh));
-    int s[3] = {m.x - cfg_.inc, m.y - cfg_.inc, m.z - cfg_.inc};
-    int e[3] = {s[0] + D_, s[1] + D_, s[2] + D_};
-    return volume_read_native(cfg_.vol, s, e, dst);
+    const int o[3] = {(int)((page >> (2 * Lc)) << sh) - inc, (int)(((page >> Lc) & msk) << sh) - inc,
+                      (int)((page & msk) << sh) - inc};
+    /* the part's planes [x0, x1) and rows [y0, y1) of the slot, every z:
+     * read as a box, it is the part's packed block as it stands */
+    int x0 = inc, x1 = inc + e, y0 = inc, y1 = inc + e, b = 0;
+    if (part == kPartXm) { x0 = 0; x1 = inc; y0 = 0; y1 = D; b = 1; }
+    else if (part == kPartXp) { x0 = inc + e; x1 = D; y0 = 0; y1 = D; b = 2; }
+    else if (part == kPartYm) { y0 = 0; y1 = inc; b = 3; }
+    else if (part == kPartYp) { y0 = inc + e; y1 = D; b = 4; }
+    const int s[3] = {o[0] + x0, o[1] + y0, o[2]}, en[3] = {o[0] + x1, o[1] + y1, o[2] + D};
+    return volume_read_native(cfg_.vol, s, en, img + geo_.off[b]);
+}
+
+void BrickCache::read_rows(uint64_t page, int parts, unsigned char* img) const {
+    const vt_volume* v = cfg_.vol;
+    const int Lc = cfg_.Lc, sh = cfg_.nLevels - cfg_.Lc, inc = cfg_.inc, D = D_;
+    const uint64_t msk = (1ull << Lc) - 1;
+    const int64_t o[3] = {(int64_t)((page >> (2 * Lc)) << sh) - inc, (int64_t)(((page >> Lc) & msk) << sh) - inc,
+                          (int64_t)((page & msk) << sh) - inc};
+    const size_t es = (size_t)esize_, row = (size_t)D * es;
+    /* z overlap of every row with the volume */
+    const int64_t z0 = std::max<int64_t>(0, o[2]), z1 = std::min<int64_t>(v->dims[2], o[2] + D);
+    const size_t zb = z1 > z0 ? (size_t)(z1 - z0) * es : 0;
+    const TierRow* const rows = rowList_[parts & kPartAll].data();
+    const size_t nr = rowList_[parts & kPartAll].size();
+    const int64_t X0 = o[0], Y0 = o[1], NX = v->dims[0], NY = v->dims[1], NZ = v->dims[2];
+    const unsigned char* const base = v->data;
+    /* the row's first voxel in the volume, or NULL outside it */
+    auto src_row = [=](const TierRow& r) -> const unsigned char* {
+        const int64_t X = X0 + r.x, Y = Y0 + r.y;
+        if (X < 0 || X >= NX || Y < 0 || Y >= NY || zb == 0) return nullptr;
+        return base + (size_t)((X * NY + Y) * NZ + z0) * es;
+    };
+    /* rows are short and far apart: prefetch PF rows ahead */
+    const size_t PF = row < 64 ? 32 : 8;
+    for (size_t i = 0; i < PF && i < nr; i++) {
+        const unsigned char* q = src_row(rows[i]);
+        if (!q) continue;
+        for (size_t c = 0; c < zb; c += 64) __builtin_prefetch(q + c);
+        __builtin_prefetch(q + zb - 1);
+    }
+    for (size_t i = 0; i < nr; i++) {
+        if (i + PF < nr) {
+            const unsigned char* q = src_row(rows[i + PF]);
+            if (q) {
+                for (size_t c = 0; c < zb; c += 64) __builtin_prefetch(q + c);
+                __builtin_prefetch(q + zb - 1);
+            }
+        }
+        unsigned char* d = img + rows[i].off;
+        const unsigned char* q = src_row(rows[i]);
+        if (!q) { memset(d, 0, row); continue; }
+        if (z0 > o[2]) memset(d, 0, (size_t)(z0 - o[2]) * es);
+        memcpy(d + (size_t)(z0 - o[2]) * es, q, zb);
+        if (z1 < o[2] + D) memset(d + (size_t)(z1 - o[2]) * es, 0, (size_t)(o[2] + D - z1) * es);
+    }
 }
 
 int BrickCache::host_threads() const { return cfg_.hostThreads > 0 ? cfg_.hostThreads : omp_get_max_threads(); }
 
 vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads,
-                                  uint64_t protectTick) {
+                                  uint64_t protectTick, const std::vector<unsigned char>* need) {
     const size_t n = bricks.size();
     hslot.assign(n, -1);
     const uint64_t callStart = protectTick ? protectTick : tick_ + 1;
     std::vector<size_t> miss;
+    /* reads: (brick index, parts to read); hits that lack a needed part
+     * read just that part */
+    std::vector<std::pair<size_t, unsigned char>> reads;
     for (size_t i = 0; i < n; i++) {
+        const unsigned char want = need ? (unsigned char)((*need)[i] | kPartM) : (unsigned char)kPartAll;
         int hs = hostIndex_[bricks[i] - pageBase_];
-        if (hs >= 0) { hslot[i] = hs; hostTick_[hs] = ++tick_; hostHits_++; }
-        else miss.push_back(i);
+        if (hs >= 0) {
+            hslot[i] = hs; hostTick_[hs] = ++tick_; hostHits_++;
+            const unsigned char lack = want & (unsigned char)~hostMask_[hs];
+            if (lack) reads.emplace_back(i, lack);
+        } else {
+            miss.push_back(i);
+        }
     }
-    if (miss.empty()) return VT_OK;
+    const size_t nfill = reads.size();
     /* victims: never-filled host slots first, then a sweep over the filled
      * ones skipping every slot touched in this call */
     size_t want = miss.size();
@@ -175,48 +383,78 @@ vt_status BrickCache::ensure_host(const std::vector<uint64_t>& bricks, std::vect
         hostBrick_[hs] = b;
         hostIndex_[b - pageBase_] = hs;
         hostTick_[hs] = ++tick_;
+        hostMask_[hs] = 0;
         hslot[miss[k]] = hs;
+        reads.emplace_back(miss[k], need ? (unsigned char)((*need)[miss[k]] | kPartM) : (unsigned char)kPartAll);
     }
+    if (reads.empty()) return VT_OK;
+    const size_t nread = reads.size();
     const auto tr = std::chrono::steady_clock::now();
-    /* each brick is gathered in a per-thread buffer that stays in cache, then
-     * streamed to its tier slot: the tier's lines are written without being
-     * read first, and do not displace the volume rows other reads share */
+    /* each brick (or part) is gathered in a per-thread buffer that stays in
+     * cache, then streamed to its tier slot: the tier's lines are written
+     * without being read first, and do not displace the volume rows other
+     * reads share */
     /* a few hundred bricks (a steady-state pass) still spread over every
      * thread */
     const int nth = host_threads();
-    const int grain = (int)std::max<size_t>(1, std::min<size_t>(8, want / ((size_t)nth * 4)));
-    std::vector<unsigned char> bad(want, 0);
+    const int grain = (int)std::max<size_t>(1, std::min<size_t>(8, nread / ((size_t)nth * 4)));
+    std::vector<unsigned char> bad(nread, 0);
     int nbad = 0;
 #pragma omp parallel num_threads(nth) reduction(+ : nbad)
     {
         static thread_local std::vector<unsigned char> stage;
-        if (stage.size() < slotBytes_) stage.resize(slotBytes_);
+        if (stage.size() < tierBytes_) stage.resize(tierBytes_);
+        unsigned char* const img = stage.data();
 #pragma omp for schedule(dynamic, grain)
-        for (long long k = 0; k < (long long)want; k++) {
-            size_t i = miss[k];
-            if (!read_brick(bricks[i], stage.data())) { bad[k] = 1; nbad++; continue; }
-            stream_copy(h_tier_ + (size_t)hslot[i] * slotBytes_, stage.data(), slotBytes_);
+        for (long long k = 0; k < (long long)nread; k++) {
+            const size_t i = reads[k].first;
+            const unsigned char parts = reads[k].second;
+            unsigned char* slot = h_tier_ + (size_t)hslot[i] * tierBytes_;
+            /* the parts' rows into a packed image in a per-thread buffer
+             * that stays in cache, then streamed to the tier slot block by
+             * block: whole aligned lines, written without being read first,
+             * not displacing the volume rows other reads share */
+            if (!cfg_.vol->reader) {
+                read_rows(bricks[i], parts, img);
+            } else {
+                bool ok = true;
+                for (int q = 0; q < 5 && ok; q++)
+                    if (parts & (1 << q)) ok = read_part(bricks[i], 1 << q, img);
+                if (!ok) { bad[k] = 1; nbad++; continue; }
+            }
+            if (parts == kPartAll) {
+                stream_copy(slot, img, tierBytes_);
+            } else {
+                for (int q = 0; q < 5; q++)
+                    if (parts & (1 << q))
+                        stream_copy(slot + geo_.off[q], img + geo_.off[q], (geo_.len[q] + 63) & ~(size_t)63);
+            }
         }
         stream_fence();
     }
     msHostRead_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tr).count();
+    for (size_t k = 0; k < nread; k++)
+        if (!bad[k]) hostMask_[hslot[reads[k].first]] |= reads[k].second;
     if (nbad) {
         /* a failed read leaves its tier slot empty again: nothing refers to
          * the brick, and the next request reads it anew */
         uint64_t first = kEmpty;
-        for (size_t k = 0; k < want; k++) {
+        for (size_t k = 0; k < nread; k++) {
             if (!bad[k]) continue;
-            const size_t i = miss[k];
+            const size_t i = reads[k].first;
             const int hs = hslot[i];
             if (first == kEmpty) first = bricks[i];
             hostIndex_[bricks[i] - pageBase_] = -1;
             hostBrick_[hs] = kEmpty;
             hostTick_[hs] = 0;
+            hostMask_[hs] = 0;
             freeHost_.push_back(hs);
             hslot[i] = -1;
         }
-        hostMisses_ += (int64_t)(want - nbad);
-        *diskLoads += (int64_t)(want - nbad);
+        int missBad = 0;
+        for (size_t k = nfill; k < nread; k++) missBad += bad[k];
+        hostMisses_ += (int64_t)(want - missBad);
+        *diskLoads += (int64_t)(want - missBad);
         return fail(VT_ERR_IO, "reading %d brick(s) from the volume failed (first: page %llu)", nbad,
                     (unsigned long long)first);
     }
@@ -233,26 +471,47 @@ vt_status BrickCache::refresh_stamps(cudaStream_t s) {
     return VT_OK;
 }
 
-vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
-                                    unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync) {
-    const size_t n = bricks.size();
-    if (n == 0) return VT_OK;
-    Xfer& X = xf_[xfNext_];
-    xfNext_ ^= 1;
-    if (X.pending) {
-        const auto tw = std::chrono::steady_clock::now();
-        CKC(cudaEventSynchronize(X.ev));
-        X.pending = false;
-        msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
+vt_status BrickCache::launch_loads(const SplitItem* d_items, size_t n, int phase, cudaStream_t s) {
+    /* grid.x stays far below its limit: a launch loads at most one item per
+     * device slot */
+    launches_++;
+    k_fill_split<<<(unsigned int)n, 256, 0, s>>>((const unsigned char*)d_tier_, d_stage_, (unsigned char*)d_slab_, geo_,
+                                                 d_items, phase);
+    CKC(cudaGetLastError());
+    return VT_OK;
+}
+
+vt_status BrickCache::stage_runs(SplitItem* items, size_t n, cudaStream_t s, double* bytes) {
+    /* the copy engine outruns SM loads from mapped memory over PCIe (55
+     * against 49 GB/s), but moves whole slots only: runs of >= 16 whole
+     * bricks in consecutive tier slots (a cold start hands tier slots out
+     * in order) go by it, into staging slots reused by the next call (a
+     * later copy on the same stream waits for this call's fill kernel) */
+    const size_t kMinRun = 16;
+    size_t used = 0;
+    for (size_t k = 0; k < n;) {
+        size_t e = k + 1;
+        if (items[k].parts == kPartAll)
+            while (e < n && items[e].parts == kPartAll && items[e].hs == items[e - 1].hs + 1) e++;
+        const size_t len = e - k;
+        if (items[k].parts == kPartAll && len >= kMinRun && used + len <= stageCap_) {
+            CKC(cudaMemcpyAsync(d_stage_ + used * tierBytes_, h_tier_ + (size_t)items[k].hs * tierBytes_,
+                                len * tierBytes_, cudaMemcpyHostToDevice, s));
+            for (size_t j = k; j < e; j++) { items[j].hs = (int)(used + (j - k)); items[j].staged = 1; }
+            used += len;
+            *bytes += (double)len * tierBytes_;
+        }
+        k = e;
     }
-    /* bricks with a host-tier copy, at most one per device slot */
-    size_t m = 0;
-    while (m < n && m < (size_t)nSlots_ && hslot[m] >= 0) m++;
-    /* slots: never-filled ones first; then a sweep over the filled slots
-     * with the kernels' stamps, first taking slots not used since the frame
-     * began, then any stamped before protectFrom (slots a kernel of the
-     * current pass used always have a newer stamp) */
-    std::vector<int> order;
+    return VT_OK;
+}
+
+vt_status BrickCache::pick_slots(size_t m, unsigned int protectFrom, cudaStream_t s, std::vector<int>& order) {
+    /* never-filled slots first; then a sweep over the filled slots with the
+     * kernels' stamps, first taking slots not used since the frame began,
+     * then any stamped before protectFrom (slots a kernel of the current
+     * pass used always have a newer stamp) */
+    order.clear();
     order.reserve(m);
     while (order.size() < m && !freeSlots_.empty()) { order.push_back(freeSlots_.back()); freeSlots_.pop_back(); }
     if (order.size() < m) {
@@ -271,6 +530,27 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
             }
         }
     }
+    return VT_OK;
+}
+
+vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
+                                    unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync) {
+    const size_t n = bricks.size();
+    if (n == 0) return VT_OK;
+    Xfer& X = xf_[xfNext_];
+    xfNext_ ^= 1;
+    if (X.pending) {
+        const auto tw = std::chrono::steady_clock::now();
+        CKC(cudaEventSynchronize(X.ev));
+        X.pending = false;
+        msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
+    }
+    /* bricks with a host-tier copy, at most one per device slot */
+    size_t m = 0;
+    while (m < n && m < (size_t)nSlots_ && hslot[m] >= 0) m++;
+    std::vector<int> order;
+    vt_status pst = pick_slots(m, protectFrom, s, order);
+    if (pst != VT_OK) return pst;
     size_t need = n * 2 + 2;
     if (need > X.ucap) {
         if (X.hu) cudaFreeHost(X.hu);
@@ -279,15 +559,15 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
         CKC(cudaHostAlloc((void**)&X.hu, X.ucap * sizeof(int2), cudaHostAllocDefault));
         CKC(cudaMalloc(&X.du, X.ucap * sizeof(int2)));
     }
-    if (n > X.pcap) {
-        if (X.hp) cudaFreeHost(X.hp);
-        cudaFree(X.dp);
-        X.pcap = n * 2;
-        CKC(cudaHostAlloc((void**)&X.hp, X.pcap * sizeof(int2), cudaHostAllocDefault));
-        CKC(cudaMalloc(&X.dp, X.pcap * sizeof(int2)));
+    if (n > X.icap) {
+        if (X.hi) cudaFreeHost(X.hi);
+        cudaFree(X.di);
+        X.icap = n * 2;
+        CKC(cudaHostAlloc((void**)&X.hi, X.icap * sizeof(SplitItem), cudaHostAllocDefault));
+        CKC(cudaMalloc(&X.di, X.icap * sizeof(SplitItem)));
     }
     int2* const h_upd_ = X.hu;
-    int2* const h_pairs_ = X.hp;
+    SplitItem* const items = X.hi;
     size_t nu = 0, np = 0;
     for (size_t k = 0; k < order.size(); k++) {
         int slot = order[k];
@@ -301,34 +581,22 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
         pageMirror_[b - pageBase_] = slot;
         stampHost_[slot] = pass_ + 1;
         h_upd_[nu++] = make_int2((int)(b - pageBase_), slot);
-        h_pairs_[np] = make_int2(hslot[np], slot);
+        SplitItem& it = items[np];
+        it.hs = hslot[np]; it.slot = slot; it.parts = kPartAll; it.staged = 0;
+        it.nb[0] = it.nb[1] = it.nb[2] = it.nb[3] = -1;
         np++;
     }
     /* requests that got no slot go back to absent (retried next pass) */
     for (size_t k = np; k < n; k++)
         if (pageMirror_[bricks[k] - pageBase_] < 0) h_upd_[nu++] = make_int2((int)(bricks[k] - pageBase_), -1);
-    /* runs of consecutive host slots going to consecutive device slots (a
-     * cold start hands out both in order) move by the copy engine, which
-     * outruns SM loads from mapped memory over PCIe; the rest by the kernel */
-    const size_t kMinRun = 16;
-    size_t nk = 0;
-    for (size_t k = 0; k < np;) {
-        size_t e = k + 1;
-        while (e < np && h_pairs_[e].x == h_pairs_[e - 1].x + 1 && h_pairs_[e].y == h_pairs_[e - 1].y + 1) e++;
-        if (e - k >= kMinRun) {
-            CKC(cudaMemcpyAsync((unsigned char*)d_slab_ + (size_t)h_pairs_[k].y * slotBytes_, h_tier_ + (size_t)h_pairs_[k].x * slotBytes_,
-                                (e - k) * slotBytes_, cudaMemcpyHostToDevice, s));
-        } else {
-            for (size_t j = k; j < e; j++) h_pairs_[nk++] = h_pairs_[j];
-        }
-        k = e;
-    }
-    if (nk) {
-        launches_++;
-        CKC(cudaMemcpyAsync(X.dp, h_pairs_, nk * sizeof(int2), cudaMemcpyHostToDevice, s));
-        k_fill_bricks<<<(unsigned int)nk, 256, 0, s>>>((const unsigned char*)d_tier_, slotBytes_, X.dp,
-                                                       (unsigned char*)d_slab_);
-        CKC(cudaGetLastError());
+    double bytes = 0;
+    if (np) {
+        vt_status lst = stage_runs(items, np, s, &bytes);
+        if (lst != VT_OK) return lst;
+        for (size_t k = 0; k < np; k++)
+            if (!items[k].staged) bytes += part_bytes(kPartAll);
+        CKC(cudaMemcpyAsync(X.di, items, np * sizeof(SplitItem), cudaMemcpyHostToDevice, s));
+        if ((lst = launch_loads(X.di, np, 1, s)) != VT_OK) return lst;
     }
     if (nu) {
         launches_++;
@@ -346,7 +614,141 @@ vt_status BrickCache::assign_device(const std::vector<uint64_t>& bricks, const s
         xf_[0].pending = xf_[1].pending = false;
         msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
     }
-    *h2d += (double)np * (double)slotBytes_;
+    *h2d += bytes;
+    *loaded += (int64_t)np;
+    return VT_OK;
+}
+
+vt_status BrickCache::load_demand(const std::vector<uint64_t>& demand, size_t cap, size_t chunk, cudaStream_t s,
+                                  uint64_t svcStart, double* h2d, int64_t* loaded, int64_t* disk) {
+    const size_t n = demand.size();
+    if (n == 0) return VT_OK;
+    /* transfers of earlier calls (lookahead, prefetch) end first: their
+     * pinned lists are not shared with this one, but their slots are */
+    for (Xfer& X : xf_)
+        if (X.pending) {
+            const auto tw = std::chrono::steady_clock::now();
+            CKC(cudaEventSynchronize(X.ev));
+            X.pending = false;
+            msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
+        }
+    std::vector<int> order;
+    vt_status st = pick_slots(std::min(cap, (size_t)nSlots_), 0xFFFFFFFFu, s, order);
+    if (st != VT_OK) return st;
+    const size_t np = order.size();
+    if (np > svcItemsCap_) {
+        if (svcItemsH_) cudaFreeHost(svcItemsH_);
+        cudaFree(svcItemsD_);
+        svcItemsCap_ = np * 2;
+        CKC(cudaHostAlloc((void**)&svcItemsH_, svcItemsCap_ * sizeof(SplitItem), cudaHostAllocDefault));
+        CKC(cudaMalloc(&svcItemsD_, svcItemsCap_ * sizeof(SplitItem)));
+    }
+    if (n + np + 2 > svcUpdCap_) {
+        if (svcUpdH_) cudaFreeHost(svcUpdH_);
+        cudaFree(svcUpdD_);
+        svcUpdCap_ = (n + np + 2) * 2;
+        CKC(cudaHostAlloc((void**)&svcUpdH_, svcUpdCap_ * sizeof(int2), cudaHostAllocDefault));
+        CKC(cudaMalloc(&svcUpdD_, svcUpdCap_ * sizeof(int2)));
+    }
+    int2* const upd = svcUpdH_;
+    size_t nu = 0;
+    /* placement first (evictions included): a neighbour counts as a source
+     * of aprons only if its slot holds it when the copies run */
+    for (size_t k = 0; k < np; k++) {
+        const int slot = order[k];
+        if (slotBrick_[slot] != kEmpty) {
+            const uint64_t old = slotBrick_[slot];
+            pageMirror_[old - pageBase_] = -1;
+            upd[nu++] = make_int2((int)(old - pageBase_), -1);
+        }
+        slotBrick_[slot] = demand[k];
+        pageMirror_[demand[k] - pageBase_] = slot;
+        stampHost_[slot] = pass_ + 1;
+    }
+    /* requests that got no slot go back to absent (retried next pass) */
+    for (size_t k = np; k < n; k++)
+        if (pageMirror_[demand[k] - pageBase_] < 0) upd[nu++] = make_int2((int)(demand[k] - pageBase_), -1);
+    /* x/y aprons: from a neighbour resident now (not one still in flight
+     * on the side stream) or placed in this service, else from the tier */
+    const int Lc = cfg_.Lc;
+    const uint64_t grid = 1ull << Lc, msk = grid - 1;
+    const bool share = sharedAprons_ && cfg_.inc <= cfg_.edge;
+    std::vector<unsigned char> need(np, (unsigned char)kPartAll);
+    SplitItem* const items = svcItemsH_;
+    bool anyX = false, anyY = false;
+    for (size_t k = 0; k < np; k++) {
+        SplitItem& it = items[k];
+        it.hs = -1; it.slot = order[k]; it.parts = kPartAll; it.staged = 0;
+        it.nb[0] = it.nb[1] = it.nb[2] = it.nb[3] = -1;
+        if (!share) continue;
+        const uint64_t p = demand[k] - pageBase_;
+        const uint64_t bx = p >> (2 * Lc), by = (p >> Lc) & msk;
+        const bool inGrid[4] = {bx > 0, bx + 1 < grid, by > 0, by + 1 < grid};
+        const uint64_t nbPage[4] = {p - (1ull << (2 * Lc)), p + (1ull << (2 * Lc)), p - (1ull << Lc), p + (1ull << Lc)};
+        const unsigned char bit[4] = {kPartXm, kPartXp, kPartYm, kPartYp};
+        unsigned char parts = kPartM;
+        for (int d = 0; d < 4; d++) {
+            const int sl = inGrid[d] ? pageMirror_[nbPage[d]] : -1;
+            if (sl >= 0 && specMark_[nbPage[d]] != 2) it.nb[d] = sl;
+            else parts |= bit[d];
+        }
+        anyX = anyX || it.nb[0] >= 0 || it.nb[1] >= 0;
+        anyY = anyY || it.nb[2] >= 0 || it.nb[3] >= 0;
+        need[k] = it.parts = parts;
+    }
+    /* host reads and tier-to-slot transfers in chunks: the reads of one
+     * chunk overlap the transfer of the one before */
+    size_t ramp = std::max<size_t>(64, chunk / 8);
+    double bytes = 0;
+    for (size_t c0 = 0, c1; c0 < np && st == VT_OK; c0 = c1) {
+        /* chunks ramp up from chunk/8 (the first chunk's reads overlap
+         * nothing) and halve over the last 2 chunks' worth of bricks (the
+         * last chunk's transfer overlaps nothing either) */
+        const size_t rem = np - c0;
+        size_t len = std::min(ramp, rem);
+        if (rem <= 2 * chunk) len = std::min(len, std::max(std::min(rem, std::max<size_t>(64, chunk / 16)), rem / 2));
+        ramp = std::min(chunk, ramp * 2);
+        c1 = c0 + len;
+        std::vector<uint64_t> head(demand.begin() + c0, demand.begin() + c1);
+        std::vector<unsigned char> hneed(need.begin() + c0, need.begin() + c1);
+        std::vector<int> hs;
+        st = ensure_host(head, hs, disk, svcStart, &hneed);
+        if (st != VT_OK) break;
+        for (size_t j = 0; j < len; j++) items[c0 + j].hs = hs[j];
+        if ((st = stage_runs(items + c0, len, s, &bytes)) != VT_OK) break;
+        for (size_t j = 0; j < len; j++)
+            if (!items[c0 + j].staged) bytes += part_bytes(need[c0 + j]);
+        CKC(cudaMemcpyAsync(svcItemsD_ + c0, items + c0, len * sizeof(SplitItem), cudaMemcpyHostToDevice, s));
+        if ((st = launch_loads(svcItemsD_ + c0, len, 1, s)) != VT_OK) break;
+    }
+    if (st == VT_OK) {
+        if (anyY && (st = launch_loads(svcItemsD_, np, 2, s)) != VT_OK) return st;
+        if (anyX && (st = launch_loads(svcItemsD_, np, 3, s)) != VT_OK) return st;
+        for (size_t k = 0; k < np; k++) upd[nu++] = make_int2((int)(demand[k] - pageBase_), order[k]);
+    } else {
+        /* nothing of this service loads (a neighbour may count on a brick
+         * whose read failed): its slots are free again, its pages absent;
+         * the evictions stand */
+        for (size_t k = 0; k < np; k++) {
+            slotBrick_[order[k]] = kEmpty;
+            pageMirror_[demand[k] - pageBase_] = -1;
+            freeSlots_.push_back(order[k]);
+            upd[nu++] = make_int2((int)(demand[k] - pageBase_), -1);
+        }
+    }
+    if (nu) {
+        launches_++;
+        CKC(cudaMemcpyAsync(svcUpdD_, upd, nu * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_page_update<<<(unsigned int)((nu + 255) / 256), 256, 0, s>>>(d_page_, svcUpdD_, (int)nu, d_stamp_, pass_ + 1);
+        CKC(cudaGetLastError());
+    }
+    /* the loads end before the next use of the service lists (and before
+     * any freed slot is handed out again) */
+    const auto tw = std::chrono::steady_clock::now();
+    CKC(cudaStreamSynchronize(s));
+    msFillWait_ += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw).count();
+    if (st != VT_OK) return st;
+    *h2d += bytes;
     *loaded += (int64_t)np;
     return VT_OK;
 }
@@ -429,16 +831,7 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
         /* in chunks: the host-tier reads of one chunk overlap the device fill
          * of the one before */
         const size_t cap = std::min<size_t>({demand.size(), (size_t)nSlots_, (size_t)nHost_});
-        for (size_t c0 = 0; c0 < cap; c0 += kChunk) {
-            const size_t c1 = std::min(cap, c0 + kChunk);
-            const bool last = c1 == cap;
-            std::vector<uint64_t> head(demand.begin() + c0, demand.begin() + c1);
-            std::vector<int> hs;
-            if ((st = ensure_host(head, hs, &disk, svcStart)) != VT_OK) return st;
-            if (last) head.insert(head.end(), demand.begin() + cap, demand.end());   /* reset to absent */
-            hs.resize(head.size(), -1);
-            if ((st = assign_device(head, hs, s, 0xFFFFFFFFu, h2dBytes, &loaded, false)) != VT_OK) return st;
-        }
+        if ((st = load_demand(demand, cap, kChunk, s, svcStart, h2dBytes, &loaded, &disk)) != VT_OK) return st;
     }
     /* speculative requests (lookahead): only into free slots or slots this
      * frame has not used, so they never evict what its rays still need;
@@ -579,6 +972,7 @@ vt_status BrickCache::drop() {
     for (int i = 0; i < nHost_; i++) freeHost_[i] = nHost_ - 1 - i;
     hostClock_ = 0;
     std::fill(hostTick_.begin(), hostTick_.end(), 0);
+    std::fill(hostMask_.begin(), hostMask_.end(), 0);
     allResident_ = false;
     return VT_OK;
 }
@@ -624,31 +1018,15 @@ vt_status BrickCache::spec_issue(const std::vector<uint64_t>& pages, int64_t* lo
         specMark_[p] = 2;
         specChunkOf_[p] = c;
         C.slots[i] = slot;
-        C.hp[i] = make_int2(hs[i], slot);
+        SplitItem& it = C.hi[i];
+        it.hs = hs[i]; it.slot = slot; it.parts = kPartAll; it.staged = 0;
+        it.nb[0] = it.nb[1] = it.nb[2] = it.nb[3] = -1;
         C.hu[i] = make_int2((int)p, slot);
     }
-    /* runs of consecutive host and device slots by the copy engine, the rest
-     * by the fill kernel; then the page entries, after the data */
-    size_t nk = 0;
-    for (size_t k = 0; k < n;) {
-        size_t e = k + 1;
-        while (e < n && C.hp[e].x == C.hp[e - 1].x + 1 && C.hp[e].y == C.hp[e - 1].y + 1) e++;
-        if (e - k >= 16) {
-            CKC(cudaMemcpyAsync((unsigned char*)d_slab_ + (size_t)C.hp[k].y * slotBytes_,
-                                h_tier_ + (size_t)C.hp[k].x * slotBytes_, (e - k) * slotBytes_, cudaMemcpyHostToDevice,
-                                specStream_));
-        } else {
-            for (size_t j = k; j < e; j++) C.hp[nk++] = C.hp[j];
-        }
-        k = e;
-    }
-    if (nk) {
-        launches_++;
-        CKC(cudaMemcpyAsync(C.dp, C.hp, nk * sizeof(int2), cudaMemcpyHostToDevice, specStream_));
-        k_fill_bricks<<<(unsigned int)nk, 256, 0, specStream_>>>((const unsigned char*)d_tier_, slotBytes_, C.dp,
-                                                                  (unsigned char*)d_slab_);
-        CKC(cudaGetLastError());
-    }
+    /* the bricks, then the page entries, after the data */
+    CKC(cudaMemcpyAsync(C.di, C.hi, n * sizeof(SplitItem), cudaMemcpyHostToDevice, specStream_));
+    st = launch_loads(C.di, n, 1, specStream_);
+    if (st != VT_OK) return st;
     launches_++;
     CKC(cudaMemcpyAsync(C.du, C.hu, n * sizeof(int2), cudaMemcpyHostToDevice, specStream_));
     k_page_update<<<(unsigned int)((n + 255) / 256), 256, 0, specStream_>>>(d_page_, C.du, (int)n, d_stamp_, pass_);

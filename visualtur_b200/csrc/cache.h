@@ -12,10 +12,19 @@
  * slots.
  * Host tier: `hostSlots` bricks in pinned, device-mapped memory with the
  * same LRU rule; misses read the brick zero-padded from the volume source
- * (FileManager::readHDF5_Voxel_Array semantics) on host threads.  Bricks
- * cross to their device slots by the copy engine where consecutive host
- * slots go to consecutive device slots, else by a fill kernel reading the
- * mapped tier.
+ * (FileManager::readHDF5_Voxel_Array semantics) on host threads.  A fill
+ * kernel reading the mapped tier moves bricks to their device slots.
+ *
+ * Shared aprons (demand loads): a slot is five parts -- the middle M
+ * (planes [inc, inc+e) x rows [inc, inc+e), every z) and the x and y
+ * aprons X-, X+ (planes [0, inc), [inc+e, D)) and Y-, Y+ (planes
+ * [inc, inc+e), rows [0, inc), [inc+e, D)).  An x or y apron is the same
+ * voxels as planes or rows of the neighbouring brick's middle, so when
+ * that neighbour is resident (or loads in the same chunk) the apron is
+ * copied from its slot on the device, and only the rest is read from the
+ * volume, written to the host tier and crosses PCIe (the tier stores a
+ * brick packed by part, TierGeo).  Host-tier slots remember which parts
+ * they hold; a later load that needs another part reads just that part.
  */
 #pragma once
 #include <cuda_runtime.h>
@@ -33,6 +42,35 @@ struct CacheConfig {
     int nLevels = 0, Lc = 0, inc = 3, edge = 0;
     int deviceSlots = 0, hostSlots = 0, hostThreads = 0;
     bool asyncSpec = true;   /* lookahead bricks load on a side stream while passes run */
+    bool sharedAprons = true;   /* demand loads copy x/y aprons from resident neighbours */
+};
+
+/* parts of a slot (bit masks; see above) */
+enum { kPartM = 1, kPartXm = 2, kPartXp = 4, kPartYm = 8, kPartYp = 16, kPartAll = 31 };
+
+/* one brick load: host-tier slot, device slot, the parts it takes from
+ * the host tier, and the device slots of the X-, X+, Y-, Y+ neighbours
+ * whose middles supply its other x/y aprons (-1: none) */
+struct SplitItem {
+    int hs, slot, parts, staged;   /* staged: hs indexes the device staging area, not the tier */
+    int nb[4];
+};
+
+/* Slot geometry.  A device slot is the D^3 box (x slowest).  A host-tier
+ * slot holds the same voxels packed by part -- M, X-, X+, Y-, Y+, each a
+ * block starting on a 64-byte line, rows in (plane, row) order -- so a
+ * load that needs some parts reads, writes and transfers only their
+ * lines. */
+struct TierGeo {
+    int D, e, inc, es;
+    unsigned long long slotBytes, tierBytes;
+    unsigned long long off[5], len[5];
+};
+
+/* a row of a slot (plane x, row y) and its offset in a packed tier slot */
+struct TierRow {
+    int x, y;
+    unsigned int off;
 };
 
 class BrickCache {
@@ -76,6 +114,7 @@ public:
      * its chunk. */
     vt_status spec_work(cudaEvent_t passDone, int64_t* loaded);
     void set_async_spec(bool on);
+    void set_shared_aprons(bool on) { sharedAprons_ = on; }
     /* pages predicted for the coming frames (already marked requested
      * speculatively on the device): queued ahead of the lookahead queue */
     void spec_hint(const unsigned int* pages, size_t n);
@@ -89,21 +128,44 @@ public:
 
 private:
     /* protectTick: host slots touched at or after this tick are not evicted
-     * (0: those touched in this call) */
+     * (0: those touched in this call); need: the parts each brick needs in
+     * the tier (NULL: all; the middle always) */
     vt_status ensure_host(const std::vector<uint64_t>& bricks, std::vector<int>& hslot, int64_t* diskLoads,
-                          uint64_t protectTick = 0);
-    /* sync = false leaves the fill running; the transfer lists are double
-     * buffered, so the next call overlaps it */
+                          uint64_t protectTick = 0, const std::vector<unsigned char>* need = nullptr);
+    /* device slots for up to m bricks: never-filled slots first, then the
+     * clock sweep over slots not used since the frame began, then any
+     * stamped before protectFrom */
+    vt_status pick_slots(size_t m, unsigned int protectFrom, cudaStream_t s, std::vector<int>& order);
+    /* the demand loads of one service: demand[0, cap) load (as many as get
+     * a device slot), the rest go back to absent.  Every brick is placed
+     * first, so a neighbour loading in the same service counts as a source
+     * of aprons; host reads and transfers then run in chunks (the reads of
+     * one overlapping the transfer of the one before), the neighbour
+     * copies once at the end. */
+    vt_status load_demand(const std::vector<uint64_t>& demand, size_t cap, size_t chunk, cudaStream_t s,
+                          uint64_t svcStart, double* h2d, int64_t* loaded, int64_t* disk);
+    /* reads `part` of a brick from the volume (caller's read function) into
+     * a packed tier image */
+    bool read_part(uint64_t page, int part, unsigned char* img) const;
+    /* reads the rows of `parts` of a brick of an in-memory volume into a
+     * packed tier image, in one pass */
+    void read_rows(uint64_t page, int parts, unsigned char* img) const;
+    /* host-tier bytes of `parts` */
+    double part_bytes(int parts) const;
+    /* loads whole bricks (with a host-tier copy, hslot >= 0) into device
+     * slots; sync = false leaves the fill running (the transfer lists are
+     * double buffered, so the next call overlaps it) */
     vt_status assign_device(const std::vector<uint64_t>& bricks, const std::vector<int>& hslot, cudaStream_t s,
                             unsigned int protectFrom, double* h2d, int64_t* loaded, bool sync = true);
-    bool read_brick(uint64_t code, void* dst) const;
     static constexpr int kSpecChunks = 8;      /* chunks in flight on the side stream */
     static constexpr size_t kSpecChunk = 512;  /* bricks per chunk: the host reads of one
                                                   outlast a pass's end by ~0.4 ms at most */
 
     CacheConfig cfg_;
     int D_ = 0, esize_ = 4;
-    size_t brickVol_ = 0, slotBytes_ = 0;
+    size_t brickVol_ = 0, slotBytes_ = 0, tierBytes_ = 0;
+    TierGeo geo_{};
+    std::vector<TierRow> rowList_[32];       /* the rows of each part mask, in (plane, row) order */
     uint64_t pageBase_ = 0; size_t pageN_ = 0;
     int* d_page_ = nullptr;
     void* d_slab_ = nullptr;
@@ -128,13 +190,25 @@ private:
     std::vector<int> freeHost_;              /* host slots never filled since init / drop */
     int hostClock_ = 0;                      /* victim sweep position over host slots */
     std::vector<uint64_t> hostTick_;
+    std::vector<unsigned char> hostMask_;    /* host slot -> parts it holds */
+    bool sharedAprons_ = true;
     uint64_t tick_ = 0;
     /* transfer lists */
     struct Xfer {
-        int2* hp = nullptr; int2* dp = nullptr; size_t pcap = 0;   /* (host slot, device slot) pairs */
         int2* hu = nullptr; int2* du = nullptr; size_t ucap = 0;   /* (page, slot) updates */
+        SplitItem* hi = nullptr; SplitItem* di = nullptr; size_t icap = 0;   /* loads */
         cudaEvent_t ev = nullptr; bool pending = false;            /* last use still on the GPU */
     } xf_[2];
+    /* a service's demand loads (all on the device until it returns) */
+    SplitItem* svcItemsH_ = nullptr; SplitItem* svcItemsD_ = nullptr; size_t svcItemsCap_ = 0;
+    int2* svcUpdH_ = nullptr; int2* svcUpdD_ = nullptr; size_t svcUpdCap_ = 0;
+    vt_status launch_loads(const SplitItem* d_items, size_t n, int phase, cudaStream_t s);
+    /* whole bricks in runs of consecutive host-tier slots cross PCIe by the
+     * copy engine into a device staging area (the fill kernel then reads
+     * them there); marks those items (pad = 1, hs = staging index) */
+    vt_status stage_runs(SplitItem* items, size_t n, cudaStream_t s, double* bytes);
+    unsigned char* d_stage_ = nullptr;     /* staging area: stageCap_ packed tier slots */
+    size_t stageCap_ = 0;
     int xfNext_ = 0;
     unsigned long long* h_req_ = nullptr; size_t reqCap_ = 0;
     /* asynchronous speculative loads */
@@ -142,7 +216,7 @@ private:
         cudaEvent_t ev = nullptr;
         std::vector<uint64_t> pages;
         std::vector<int> slots, hslots;
-        int2* hp = nullptr; int2* dp = nullptr;   /* (host slot, device slot) pairs */
+        SplitItem* hi = nullptr; SplitItem* di = nullptr;   /* loads */
         int2* hu = nullptr; int2* du = nullptr;   /* page updates */
         size_t cap = 0;
     };

@@ -360,6 +360,7 @@ extern "C" void vt_default_options(vt_options* o) {
     o->pool_per_ray = 0;
     o->spec_async = 1;
     o->wavefront = 0;
+    o->shared_aprons = 1;
 }
 
 static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
@@ -416,6 +417,7 @@ static vt_status init_handle(vt_handle* h) {
         cc.deviceSlots = p.maxElementsCache; cc.hostSlots = p.maxElementsCache_CPU;
         cc.hostThreads = h->opt.host_threads;
         cc.asyncSpec = h->opt.spec_async != 0;
+    cc.sharedAprons = h->opt.shared_aprons != 0;
         h->cache = new vtrt::BrickCache();
         if ((s = h->cache->init(cc)) != VT_OK) return s;
         if (h->opt.preload && (size_t)p.maxElementsCache >= h->leafBricks.size()) {
@@ -537,6 +539,7 @@ extern "C" vt_status vt_change_cache(vt_handle* h, int nE, const int cDim[3], in
     cc.vol = h->vol; cc.nLevels = h->nLevels; cc.Lc = h->Lc; cc.inc = h->inc; cc.edge = h->edge;
     cc.deviceSlots = nE; cc.hostSlots = h->p.maxElementsCache_CPU; cc.hostThreads = h->opt.host_threads;
     cc.asyncSpec = h->opt.spec_async != 0;
+    cc.sharedAprons = h->opt.shared_aprons != 0;
     h->cache = new vtrt::BrickCache();
     if ((s = h->cache->init(cc)) != VT_OK) return s;
     if (h->opt.preload && (size_t)nE >= h->leafBricks.size() &&
@@ -946,12 +949,16 @@ extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
     o.skip = t->skip;
     o.spec_async = t->spec_async;
     o.wavefront = t->wavefront;
+    o.shared_aprons = t->shared_aprons;
     vt_status s = validate(&h->p, h->oct, &o);
     if (s != VT_OK) return s;
     if (o.lookahead < 0 || o.lookahead > 64 || o.pops < 1 || o.blocks_per_sm < 1 || o.blocks_per_sm > 32)
         return fail(VT_ERR_INVALID, "lookahead 0..64, pops >= 1, blocks_per_sm 1..32");
     h->opt = o;
-    if (h->cache) h->cache->set_async_spec(o.spec_async != 0);
+    if (h->cache) {
+        h->cache->set_async_spec(o.spec_async != 0);
+        h->cache->set_shared_aprons(o.shared_aprons != 0);
+    }
     return VT_OK;
 }
 
@@ -964,6 +971,7 @@ extern "C" vt_status vt_get_tuning(vt_handle* h, vt_tuning* t) {
     t->skip = h->opt.skip;
     t->spec_async = h->opt.spec_async;
     t->wavefront = h->opt.wavefront;
+    t->shared_aprons = h->opt.shared_aprons;
     return VT_OK;
 }
 

@@ -5,6 +5,7 @@
  */
 #include <fcntl.h>
 #include <stdarg.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -111,9 +112,21 @@ void stream_copy(void* dst, const void* src, size_t bytes) {
     for (size_t i = 0; i < bytes / 16; i++) _mm_stream_si128(d + i, _mm_loadu_si128(q + i));
 }
 void stream_fence() { _mm_sfence(); }
+void stream_copy_any(void* dst, const void* src, size_t bytes) {
+    unsigned char* d = (unsigned char*)dst;
+    const unsigned char* q = (const unsigned char*)src;
+    size_t head = (16 - ((uintptr_t)d & 15)) & 15;
+    if (head > bytes) head = bytes;
+    memcpy(d, q, head);
+    d += head; q += head; bytes -= head;
+    const size_t nw = bytes / 16;
+    for (size_t i = 0; i < nw; i++) _mm_stream_si128((__m128i*)d + i, _mm_loadu_si128((const __m128i*)q + i));
+    memcpy(d + nw * 16, q + nw * 16, bytes - nw * 16);
+}
 #else
 void stream_copy(void* dst, const void* src, size_t bytes) { memcpy(dst, src, bytes); }
 void stream_fence() {}
+void stream_copy_any(void* dst, const void* src, size_t bytes) { memcpy(dst, src, bytes); }
 #endif
 bool volume_read_native(const vt_volume* v, const int s[3], const int e[3], void* out) {
     if (v->reader) return v->reader(v->user, s, e, out) == 0;

@@ -61,6 +61,9 @@ bool volume_read_native(const vt_volume* v, const int s[3], const int e[3], void
  * thread ends its run of such copies with stream_fence() */
 void stream_copy(void* dst, const void* src, size_t bytes);
 void stream_fence();
+/* the same for any alignment and size (the unaligned head and tail by
+ * ordinary stores) */
+void stream_copy_any(void* dst, const void* src, size_t bytes);
 /* reference device-variant child membership (src/Octree.cu:375-532) */
 int children_mask(const uint64_t* e, int size, uint64_t father);
 /* reference host-variant child count (src/CreateOctree.cu:247-284) */
