@@ -806,8 +806,8 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
     launch amortises launches and host work but needs their joint working
     set in the device cache, and hints help only while the cache has room
     for them -- a small cache thrashes, which only a cold-cache run shows."""
-    def run(b, la, thr, sk=0):
-        wl.r.set_tuning(lookahead=la, skip=sk)
+    def run(b, la, thr, sk=0, sa=SHARED_APRONS):
+        wl.r.set_tuning(lookahead=la, skip=sk, shared_aprons=sa)
         L = make_launcher(wl, wl.r, cfg, torch, dev, stream, b, predictor=P)
         L.thr = thr
         wl.r.drop_cache()
@@ -822,9 +822,10 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
             e.record(stream)
             torch.cuda.synchronize()
         ms = a.elapsed_time(e)
-        log("autotune: %d frames/launch, lookahead %d, hints %s, skip %d -> %.1f ms for %d frames" %
-            (b, la, thr, sk, ms, frames))
-        return {"frames_per_launch": b, "lookahead": la, "hint_threshold": thr, "skip": sk, "ms": round(ms, 2)}
+        log("autotune: %d frames/launch, lookahead %d, hints %s, skip %d, shared aprons %d -> %.1f ms for %d frames" %
+            (b, la, thr, sk, sa, ms, frames))
+        return {"frames_per_launch": b, "lookahead": la, "hint_threshold": thr, "skip": sk, "shared_aprons": sa,
+                "ms": round(ms, 2)}
 
     thr0 = 0.5 if P is not None else None
     rows = [run(b, la, thr0, sk) for b, la, sk in PAGING_CANDIDATES]
@@ -835,7 +836,12 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
     if best["skip"]:
         rows.append(run(best["frames_per_launch"], best["lookahead"], best["hint_threshold"], 2))
         best = min(rows, key=lambda x: x["ms"])
-    wl.r.set_tuning(lookahead=best["lookahead"], skip=best["skip"])
+    if SHARED_APRONS:
+        # under eviction churn a brick loaded without its x/y aprons may have
+        # to read them later (its neighbours gone): whole bricks can win
+        rows.append(run(best["frames_per_launch"], best["lookahead"], best["hint_threshold"], best["skip"], 0))
+        best = min(rows, key=lambda x: x["ms"])
+    wl.r.set_tuning(lookahead=best["lookahead"], skip=best["skip"], shared_aprons=best["shared_aprons"])
     wl.r.drop_cache()
     return best, rows
 
@@ -943,6 +949,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
         L.thr = paging["best"]["hint_threshold"]
     skip_used = wl.r.tuning()["skip"]
     wave_used = wl.r.tuning()["wavefront"]
+    aprons_used = wl.r.tuning()["shared_aprons"]
     e2e_raw = {}
     ms, per, launches, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index),
                                           cfg["l2flush"], e2e=e2e_raw)
@@ -1028,7 +1035,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
         conf = {"W": W, "H": H, "frames_per_launch": batch, "skip": skip_used,
                 "wavefront": wave_used}
     if not cfg["resident"]:
-        conf["shared_aprons"] = SHARED_APRONS
+        conf["shared_aprons"] = aprons_used
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {

@@ -29,38 +29,48 @@ namespace vtrt {
         if (e_ != cudaSuccess) return fail(VT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
-/* Warp-cooperative copy of n bytes: 16-byte words where source and
- * destination agree modulo 16, else 4-byte words where they agree modulo
- * 4, else bytes; four words in flight per lane (loads from mapped host
- * memory cross PCIe). */
-template <typename W>
-__device__ __forceinline__ void warp_copy_w(unsigned char* d, const unsigned char* q, size_t n, int lane) {
-    const size_t a = sizeof(W);
-    size_t head = (a - ((size_t)d & (a - 1))) & (a - 1);
-    if (head > n) head = n;
-    if ((size_t)lane < head) d[lane] = q[lane];
-    d += head; q += head; n -= head;
-    const size_t nw = n / a;
-    W* dw = (W*)d;
-    const W* qw = (const W*)q;
-    for (size_t i = lane; i < nw; i += 128) {
-        W v0 = qw[i], v1, v2, v3;
-        if (i + 32 < nw) v1 = qw[i + 32];
-        if (i + 64 < nw) v2 = qw[i + 64];
-        if (i + 96 < nw) v3 = qw[i + 96];
-        dw[i] = v0;
-        if (i + 32 < nw) dw[i + 32] = v1;
-        if (i + 64 < nw) dw[i + 64] = v2;
-        if (i + 96 < nw) dw[i + 96] = v3;
+/* Warp-cooperative copy of n bytes through this warp's shared buffer
+ * (kCopyBuf bytes): the source is read in aligned 16-byte words whatever
+ * its alignment (loads from mapped host memory cross PCIe, so they must be
+ * wide), four words in flight per lane; the destination is written in
+ * 4-byte words assembled with byte permutes, bytes at its unaligned ends.
+ * The aligned words may reach up to 15 bytes before and after the range:
+ * every caller copies within a 16-byte aligned slot. */
+constexpr int kCopyBuf = 2048;
+__device__ __forceinline__ void warp_copy(unsigned char* dst, const unsigned char* src, size_t n, int lane,
+                                          unsigned int* buf) {
+    const int sa = (int)((size_t)src & 15);
+    const uint4* s16 = (const uint4*)(src - sa);
+    const size_t piece = kCopyBuf - 16;
+    const unsigned char* sb = (const unsigned char*)buf;
+    for (size_t b0 = 0; b0 < n; b0 += piece) {
+        const int len = (int)min(piece, n - b0);
+        const int words = (sa + len + 15) >> 4;
+        const uint4* sw = s16 + (b0 >> 4);
+        for (int i = lane; i < words; i += 128) {
+            uint4 v0 = sw[i], v1, v2, v3;
+            if (i + 32 < words) v1 = sw[i + 32];
+            if (i + 64 < words) v2 = sw[i + 64];
+            if (i + 96 < words) v3 = sw[i + 96];
+            ((uint4*)buf)[i] = v0;
+            if (i + 32 < words) ((uint4*)buf)[i + 32] = v1;
+            if (i + 64 < words) ((uint4*)buf)[i + 64] = v2;
+            if (i + 96 < words) ((uint4*)buf)[i + 96] = v3;
+        }
+        __syncwarp();
+        unsigned char* d = dst + b0;
+        const int head = min((int)((4 - ((size_t)d & 3)) & 3), len);
+        if (lane < head) d[lane] = sb[sa + lane];
+        const int nw = (len - head) >> 2;
+        unsigned int* dw = (unsigned int*)(d + head);
+        for (int j = lane; j < nw; j += 32) {
+            const int p = sa + head + 4 * j;
+            dw[j] = __byte_perm(buf[p >> 2], buf[(p >> 2) + 1], 0x3210 + 0x1111 * (p & 3));
+        }
+        const int t = head + 4 * nw;
+        if (lane < len - t) d[t + lane] = sb[sa + t + lane];
+        __syncwarp();
     }
-    const size_t t = nw * a;
-    if ((size_t)lane < n - t) d[t + lane] = q[t + lane];
-}
-__device__ __forceinline__ void warp_copy(unsigned char* d, const unsigned char* q, size_t n, int lane) {
-    const size_t x = (size_t)d ^ (size_t)q;
-    if ((x & 15) == 0) warp_copy_w<uint4>(d, q, n, lane);
-    else if ((x & 3) == 0) warp_copy_w<unsigned int>(d, q, n, lane);
-    else warp_copy_w<unsigned char>(d, q, n, lane);
 }
 
 /* Brick loads, one CTA per brick, in up to three launches on one stream:
@@ -71,8 +81,10 @@ __device__ __forceinline__ void warp_copy(unsigned char* d, const unsigned char*
 __global__ void k_fill_split(const unsigned char* __restrict__ tier, const unsigned char* __restrict__ stage,
                              unsigned char* __restrict__ slab, TierGeo g, const SplitItem* __restrict__ items,
                              int phase) {
+    __shared__ __align__(16) unsigned int cbuf[8][kCopyBuf / 4];
     const SplitItem it = items[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    unsigned int* const buf = cbuf[warp];
     const int e = g.e, inc = g.inc;
     unsigned char* dst = slab + (size_t)it.slot * g.slotBytes;
     const size_t row = (size_t)g.D * g.es, plane = (size_t)g.D * row;
@@ -98,7 +110,7 @@ __global__ void k_fill_split(const unsigned char* __restrict__ tier, const unsig
                 doff = (size_t)(inc + q) * plane + (lo ? 0 : (size_t)(inc + e) * row);
                 len = (size_t)inc * row;
             }
-            if (it.parts & (1 << b)) warp_copy(dst + doff, src + soff, len, lane);
+            if (it.parts & (1 << b)) warp_copy(dst + doff, src + soff, len, lane, buf);
         }
     } else if (phase == 2) {
         /* Y-: rows [0, inc) = the (y-1) neighbour's rows [e, e+inc); Y+: rows
@@ -110,7 +122,7 @@ __global__ void k_fill_split(const unsigned char* __restrict__ tier, const unsig
             const int p = lo ? c : c - e;
             const size_t doff = (size_t)(inc + p) * plane + (lo ? 0 : (size_t)(inc + e) * row);
             const size_t soff = lo ? doff + (size_t)e * row : doff - (size_t)e * row;
-            warp_copy(dst + doff, slab + (size_t)nb * g.slotBytes + soff, (size_t)inc * row, lane);
+            warp_copy(dst + doff, slab + (size_t)nb * g.slotBytes + soff, (size_t)inc * row, lane, buf);
         }
     } else {
         /* X-: planes [0, inc) = the (x-1) neighbour's planes [e, e+inc); X+:
@@ -122,7 +134,7 @@ __global__ void k_fill_split(const unsigned char* __restrict__ tier, const unsig
             const int q = lo ? c : c - inc;
             const size_t doff = (size_t)(lo ? q : inc + e + q) * plane;
             const size_t soff = (size_t)(lo ? e + q : inc + q) * plane;
-            warp_copy(dst + doff, slab + (size_t)nb * g.slotBytes + soff, plane, lane);
+            warp_copy(dst + doff, slab + (size_t)nb * g.slotBytes + soff, plane, lane, buf);
         }
     }
 }
@@ -190,6 +202,7 @@ vt_status BrickCache::init(const CacheConfig& c) {
          * their packed offsets */
         if (tierBytes_ > 0xFFFFFFFFull) return fail(VT_ERR_INVALID, "brick too large");
         const int D = D_, e = c.edge, inc = c.inc;
+        const long long NY = c.vol->dims[1], NZ = c.vol->dims[2];
         for (int parts = 0; parts < 32; parts++) {
             std::vector<TierRow>& L = rowList_[parts];
             L.clear();
@@ -198,7 +211,8 @@ vt_status BrickCache::init(const CacheConfig& c) {
                     const bool lo = x < inc;
                     if (!(parts & (lo ? kPartXm : kPartXp))) continue;
                     const size_t base = g.off[lo ? 1 : 2] + (size_t)(lo ? x : x - inc - e) * D * row;
-                    for (int y = 0; y < D; y++) L.push_back({x, y, (unsigned int)(base + (size_t)y * row)});
+                    for (int y = 0; y < D; y++)
+                        L.push_back({x, y, (unsigned int)(base + (size_t)y * row), ((long long)x * NY + y) * NZ});
                     continue;
                 }
                 const int p = x - inc;
@@ -214,7 +228,7 @@ vt_status BrickCache::init(const CacheConfig& c) {
                         if (!(parts & kPartM)) continue;
                         o2 = g.off[0] + ((size_t)p * e + (y - inc)) * row;
                     }
-                    L.push_back({x, y, (unsigned int)o2});
+                    L.push_back({x, y, (unsigned int)o2, ((long long)x * NY + y) * NZ});
                 }
             }
         }
@@ -317,6 +331,24 @@ void BrickCache::read_rows(uint64_t page, int parts, unsigned char* img) const {
     };
     /* rows are short and far apart: prefetch PF rows ahead */
     const size_t PF = row < 64 ? 32 : 8;
+    if (X0 >= 0 && Y0 >= 0 && o[2] >= 0 && X0 + D <= NX && Y0 + D <= NY && o[2] + D <= NZ) {
+        /* the slot lies inside the volume: every row is whole */
+        const unsigned char* const first = base + (size_t)((X0 * NY + Y0) * NZ + o[2]) * es;
+        for (size_t i = 0; i < PF && i < nr; i++) {
+            const unsigned char* q = first + rows[i].src * (long long)es;
+            for (size_t c = 0; c < row; c += 64) __builtin_prefetch(q + c);
+            __builtin_prefetch(q + row - 1);
+        }
+        for (size_t i = 0; i < nr; i++) {
+            if (i + PF < nr) {
+                const unsigned char* q = first + rows[i + PF].src * (long long)es;
+                for (size_t c = 0; c < row; c += 64) __builtin_prefetch(q + c);
+                __builtin_prefetch(q + row - 1);
+            }
+            memcpy(img + rows[i].off, first + rows[i].src * (long long)es, row);
+        }
+        return;
+    }
     for (size_t i = 0; i < PF && i < nr; i++) {
         const unsigned char* q = src_row(rows[i]);
         if (!q) continue;

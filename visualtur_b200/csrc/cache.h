@@ -67,10 +67,13 @@ struct TierGeo {
     unsigned long long off[5], len[5];
 };
 
-/* a row of a slot (plane x, row y) and its offset in a packed tier slot */
+/* a row of a slot (plane x, row y), its offset in a packed tier slot and,
+ * for an in-memory volume, the offset of its first voxel from the slot's
+ * first voxel in the volume (in voxels) */
 struct TierRow {
     int x, y;
     unsigned int off;
+    long long src;
 };
 
 class BrickCache {
