@@ -794,6 +794,7 @@ PAGING_CANDIDATES = ((8, 2, 0), (4, 2, 0), (2, 2, 0), (1, 2, 0), (1, 0, 0),
                      (8, 0, 0), (4, 0, 0), (2, 0, 0), (4, 1, 0),
                      (4, 2, 4), (2, 2, 4), (4, 0, 4), (2, 0, 4), (1, 0, 4), (4, 0, 2))
 HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
+DEMAND_BATCHES = (8192,)                                        # besides 0 = no bound
 VIEWS_PAGING = ((2, 0), (0, 0), (2, 2), (0, 2))                 # batched views: (lookahead, skip)
 
 
@@ -806,8 +807,8 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
     launch amortises launches and host work but needs their joint working
     set in the device cache, and hints help only while the cache has room
     for them -- a small cache thrashes, which only a cold-cache run shows."""
-    def run(b, la, thr, sk=0, sa=SHARED_APRONS):
-        wl.r.set_tuning(lookahead=la, skip=sk, shared_aprons=sa)
+    def run(b, la, thr, sk=0, sa=SHARED_APRONS, db=0):
+        wl.r.set_tuning(lookahead=la, skip=sk, shared_aprons=sa, demand_batch=db)
         L = make_launcher(wl, wl.r, cfg, torch, dev, stream, b, predictor=P)
         L.thr = thr
         wl.r.drop_cache()
@@ -822,10 +823,10 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
             e.record(stream)
             torch.cuda.synchronize()
         ms = a.elapsed_time(e)
-        log("autotune: %d frames/launch, lookahead %d, hints %s, skip %d, shared aprons %d -> %.1f ms for %d frames" %
-            (b, la, thr, sk, sa, ms, frames))
+        log("autotune: %d frames/launch, lookahead %d, hints %s, skip %d, shared aprons %d, demand batch %d "
+            "-> %.1f ms for %d frames" % (b, la, thr, sk, sa, db, ms, frames))
         return {"frames_per_launch": b, "lookahead": la, "hint_threshold": thr, "skip": sk, "shared_aprons": sa,
-                "ms": round(ms, 2)}
+                "demand_batch": db, "ms": round(ms, 2)}
 
     thr0 = 0.5 if P is not None else None
     rows = [run(b, la, thr0, sk) for b, la, sk in PAGING_CANDIDATES]
@@ -841,7 +842,15 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
         # to read them later (its neighbours gone): whole bricks can win
         rows.append(run(best["frames_per_launch"], best["lookahead"], best["hint_threshold"], best["skip"], 0))
         best = min(rows, key=lambda x: x["ms"])
-    wl.r.set_tuning(lookahead=best["lookahead"], skip=best["skip"], shared_aprons=best["shared_aprons"])
+    if wl.r.tuning()["spec_async"]:
+        # a cold start's demand bricks past a batch load on the side stream
+        # while the next pass runs
+        for db in DEMAND_BATCHES:
+            rows.append(run(best["frames_per_launch"], best["lookahead"], best["hint_threshold"], best["skip"],
+                            best["shared_aprons"], db))
+        best = min(rows, key=lambda x: x["ms"])
+    wl.r.set_tuning(lookahead=best["lookahead"], skip=best["skip"], shared_aprons=best["shared_aprons"],
+                    demand_batch=best["demand_batch"])
     wl.r.drop_cache()
     return best, rows
 
@@ -936,12 +945,16 @@ def run_ours(args, cfg, rank, world, torch, dist):
         wl.r.set_tuning(skip=args.skip)
     if not cfg["resident"]:
         wl.r.set_tuning(spec_async=args.spec_async, wavefront=args.wavefront)
+        if args.demand_batch is not None:
+            wl.r.set_tuning(demand_batch=args.demand_batch)
     if M["autotune"] and not args.no_autotune:
         tune = autotune(args, wl, cfg, torch, dev, stream, frame0, batch)
         if args.skip is not None:      # the brick sweep may have built a new renderer
             wl.r.set_tuning(skip=args.skip)
         if not cfg["resident"]:
             wl.r.set_tuning(spec_async=args.spec_async, wavefront=args.wavefront)
+            if args.demand_batch is not None:
+                wl.r.set_tuning(demand_batch=args.demand_batch)
     if P is not None:
         P.set_bricks(wl.r.brick_list(), wl.oc.nLevels - int(round(math.log2(wl.brick))))
     L = make_launcher(wl, wl.r, cfg, torch, dev, stream, batch, predictor=P, warm=args.warm)
@@ -950,6 +963,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     skip_used = wl.r.tuning()["skip"]
     wave_used = wl.r.tuning()["wavefront"]
     aprons_used = wl.r.tuning()["shared_aprons"]
+    batch_used = wl.r.tuning()["demand_batch"]
     e2e_raw = {}
     ms, per, launches, clk = timed_frames(L, frame0, args.warmup, args.steps, dist, Clocks(dev.index),
                                           cfg["l2flush"], e2e=e2e_raw)
@@ -1036,6 +1050,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
                 "wavefront": wave_used}
     if not cfg["resident"]:
         conf["shared_aprons"] = aprons_used
+        conf["demand_batch"] = batch_used
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
@@ -1204,6 +1219,9 @@ def main():
     ap.add_argument("--skip", type=int, default=None,
                     help="absent-brick candidates a ray may set aside per pass (default: tuned on fly-throughs, 0 on "
                          "batched views)")
+    ap.add_argument("--demand-batch", type=int, default=None,
+                    help="fixed demand batch (bricks a service loads itself before queuing the rest on the side "
+                         "stream; 0: no bound) instead of the tuner's choice")
     ap.add_argument("--shared-aprons", type=int, default=1, choices=(0, 1),
                     help="1: demand loads copy x/y aprons from resident neighbours' slots; 0: whole bricks")
     args = ap.parse_args()

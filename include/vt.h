@@ -230,6 +230,11 @@ typedef struct {
      * and transfers only the rest; 0: every load reads and transfers the
      * whole brick.  Same bricks either way. */
     int shared_aprons;
+    /* with spec_async: a pass's service loads at most this many demand
+     * bricks itself while never-filled slots can take them all (a cold
+     * start) and hands the rest to the side stream, which loads them while
+     * the next pass runs (0: no bound).  Same images. */
+    int demand_batch;
 } vt_options;
 
 typedef struct vt_handle vt_handle;
@@ -259,10 +264,10 @@ vt_status vt_change_cache(vt_handle* h, int maxElements, const int cubeDim[3], i
  * march unroll, persistent ray queue, traversal steps between refills,
  * persistent CTAs per SM, lookahead requests, graph replay, absent-brick
  * candidates set aside per pass, side-stream lookahead loads, wavefront
- * rounds, shared aprons. */
+ * rounds, shared aprons, demand batch. */
 typedef struct {
     int tile_w, tile_h, unroll, persistent, pops, blocks_per_sm, lookahead, use_graph, skip, spec_async, wavefront,
-        shared_aprons;
+        shared_aprons, demand_batch;
 } vt_tuning;
 vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t);
 vt_status vt_get_tuning(vt_handle* h, vt_tuning* t);

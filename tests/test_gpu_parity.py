@@ -350,3 +350,35 @@ def test_side_stream_lookahead_loads_keep_pixels(case, workdir, cuda):
     st = r.stats()
     assert st["bricks_speculative"] > 0 and st["bricks_spec_loaded"] > 0
     r.close()
+
+
+@pytest.mark.parametrize("case", ["c1", "s64rot"])
+def test_deferred_demand_loads_keep_pixels(case, workdir, cuda):
+    """A service that loads only a few demand bricks itself (demand_batch)
+    and hands the rest to the cache's side stream, which loads them while
+    the next pass runs: rays that find them absent request them again, and
+    every frame equals the oracle's."""
+    c = F.CASES[case]
+    vol = F.case_volume(case)
+    fm, oc = vt.FileManager.wrap(vol), vt.Octree(F.case_octree(case, workdir))
+    nb = 8 ** c["levelC"]
+    p = vt.make_params(W=c["W"], H=c["H"], octreeFile=None, hdf5File=None, octreeLevel=c["levelO"],
+                       levelCubes=c["levelC"], dimCube=1 << (int(np.log2(c["n"])) - c["levelC"]),
+                       cubeInc=c["inc"], distance=c["dist"], fov_H=c["fov"], fov_W=c["fov"],
+                       maxElementsCache=nb, maxElementsCache_CPU=nb)
+    r = vt.visualTur(p, vt.default_options(resident=0, preload=0, record_hits=1, persistent=1, lookahead=0,
+                                           pops=3, spec_async=1, demand_batch=4, max_passes=100000),
+                     volume=fm, octree=oc)
+    m = {"mv": r.camera_Move, "rx": r.camera_RotateX, "ry": r.camera_RotateY, "rz": r.camera_RotateZ,
+         "mf": r.camera_MoveForward, "mu": r.camera_MoveUpward, "sr": r.camera_StrafeRight}
+    for op, v in c["ops"]:
+        m[op](v)
+    for k, extra in enumerate([(), (("ry", 4.0),), (("ry", 4.0), ("rx", 3.0))]):
+        if k:
+            op, v = extra[-1]
+            m[op](v)
+        rgba, rgb8 = r.render_host()
+        node, brick, t, nrm = r.debug_hits()
+        a = dict(rgba=rgba, rgb8=rgb8, node=node, brick=brick, t=t, normal=nrm)
+        assert_parity(a, oracle_render(case, workdir, extra_ops=extra))
+    r.close()

@@ -61,6 +61,7 @@ def decode(code, Lc):
     (np.float32, 4, 3, 60, {"shared_aprons": 0}),                  # whole bricks only
     (np.uint8, 4, 3, 4096, {"spec_async": 0}),                     # lookahead with the demand loads
     (np.float32, 3, 3, 200, {"spec_async": 0, "lookahead": 0}),    # 16^3 bricks, demand loads only
+    (np.float32, 4, 3, 4096, {"lookahead": 0, "demand_batch": 8}),  # most demand bricks via the side stream
 ])
 def test_slots_hold_the_padded_box(dtype, levelC, inc, dev, opts, tmp_path, cuda):
     vol, iso = volume(dtype)

@@ -51,7 +51,7 @@ class vt_options(C.Structure):
                                          "host_threads", "record_trace", "trace_level", "record_hits",
                                          "persistent", "blocks_per_sm", "pops", "preload", "use_graph", "refine",
                                          "skip", "max_suspended", "max_requests", "pool_per_ray", "spec_async",
-                                         "wavefront", "shared_aprons")]
+                                         "wavefront", "shared_aprons", "demand_batch")]
 
 
 class vt_stats(C.Structure):
@@ -77,7 +77,7 @@ class vt_h5_info(C.Structure):
 class vt_tuning(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("tile_w", "tile_h", "unroll", "persistent", "pops", "blocks_per_sm",
                                          "lookahead", "use_graph", "skip", "spec_async", "wavefront",
-                                         "shared_aprons")]
+                                         "shared_aprons", "demand_batch")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -164,6 +164,7 @@ BrickCache::~BrickCache() {
         cudaFree(C.di); cudaFree(C.du);
     }
     if (specStream_) cudaStreamDestroy(specStream_);
+    if (svcEv_) cudaEventDestroy(svcEv_);
     cudaFree(d_page_); cudaFree(d_slab_); cudaFree(d_stamp_); cudaFree(d_stage_);
     if (h_tier_) cudaFreeHost(h_tier_);
     for (Xfer& X : xf_) {
@@ -259,6 +260,8 @@ vt_status BrickCache::init(const CacheConfig& c) {
     hostTick_.assign(nHost_, 0);
     hostMask_.assign(nHost_, 0);
     sharedAprons_ = c.sharedAprons;
+    demandBatch_ = c.demandBatch > 0 ? c.demandBatch : 0;
+    CKC(cudaEventCreateWithFlags(&svcEv_, cudaEventDisableTiming));
     slotBusy_.assign(nSlots_, 0);
     hostBusy_.assign(nHost_, 0);
     asyncSpec_ = c.asyncSpec;
@@ -846,6 +849,17 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
     std::sort(spec.begin(), spec.end());
     int64_t disk = 0, loaded = 0;
     vt_status st;
+    /* a cold start's large demand list: the first demandBatch_ bricks load
+     * now, the rest go back to "requested speculatively" and to the front of
+     * the side stream's queue -- they load into never-filled slots while the
+     * next pass runs, and a ray that still finds one absent requests it
+     * again (then it loads with the demand) */
+    std::vector<uint64_t> deferred;
+    if (asyncSpec_ && demandBatch_ > 0 && demand.size() > (size_t)demandBatch_ &&
+        freeSlots_.size() >= demand.size() && specQueued_ + demand.size() <= (size_t)nSlots_) {
+        deferred.assign(demand.begin() + demandBatch_, demand.end());
+        demand.resize(demandBatch_);
+    }
     /* chunk size: large services in chunks of 4 096 bricks (the first
      * chunk's reads and the last one's transfer are not overlapped: 8 192
      * left 6 ms of transfer waiting at the end of the c2 cold start, 4 096
@@ -864,6 +878,32 @@ vt_status BrickCache::service(const unsigned long long* d_req, unsigned int nReq
          * of the one before */
         const size_t cap = std::min<size_t>({demand.size(), (size_t)nSlots_, (size_t)nHost_});
         if ((st = load_demand(demand, cap, kChunk, s, svcStart, h2dBytes, &loaded, &disk)) != VT_OK) return st;
+    }
+    if (!deferred.empty()) {
+        const size_t nd = deferred.size();
+        if (nd + 2 > svcUpdCap_) {
+            if (svcUpdH_) cudaFreeHost(svcUpdH_);
+            cudaFree(svcUpdD_);
+            svcUpdCap_ = (nd + 2) * 2;
+            CKC(cudaHostAlloc((void**)&svcUpdH_, svcUpdCap_ * sizeof(int2), cudaHostAllocDefault));
+            CKC(cudaMalloc(&svcUpdD_, svcUpdCap_ * sizeof(int2)));
+        }
+        for (size_t k = 0; k < nd; k++) {
+            const uint64_t p = deferred[k] - pageBase_;
+            svcUpdH_[k] = make_int2((int)p, VT_PAGE_SPECULATIVE);
+            specMark_[p] = 1;
+            hintQ_.push_back(deferred[k]);
+            specQueued_++;
+        }
+        deferred_ += (int64_t)nd;
+        launches_++;
+        CKC(cudaMemcpyAsync(svcUpdD_, svcUpdH_, nd * sizeof(int2), cudaMemcpyHostToDevice, s));
+        k_page_update<<<(unsigned int)((nd + 255) / 256), 256, 0, s>>>(d_page_, svcUpdD_, (int)nd, d_stamp_, pass_ + 1);
+        CKC(cudaGetLastError());
+        CKC(cudaEventRecord(svcEv_, s));
+        /* the list's pinned copy is reused by the next service: the copy must
+         * have left it */
+        CKC(cudaStreamSynchronize(s));
     }
     /* speculative requests (lookahead): only into free slots or slots this
      * frame has not used, so they never evict what its rays still need;
@@ -1018,9 +1058,11 @@ void BrickCache::spec_poll(bool wait) {
         for (size_t i = 0; i < C.pages.size(); i++) {
             const uint64_t p = C.pages[i] - pageBase_;
             if (specMark_[p] == 2 && specChunkOf_[p] == chunkLive_[done]) { specMark_[p] = 0; specChunkOf_[p] = -1; }
-            slotBusy_[C.slots[i]] = 0;
+            slotBusy_[C.slots[i]]--;
             hostBusy_[C.hslots[i]] = 0;
         }
+        for (int sl : C.sources) slotBusy_[sl]--;
+        C.sources.clear();
         chunkFree_.push_back(chunkLive_[done]);
     }
     chunkLive_.erase(chunkLive_.begin(), chunkLive_.begin() + done);
@@ -1031,13 +1073,11 @@ vt_status BrickCache::spec_issue(const std::vector<uint64_t>& pages, int64_t* lo
     chunkFree_.pop_back();
     SpecChunk& C = chunks_[c];
     const size_t n = pages.size();
-    std::vector<int> hs;
-    int64_t disk = 0;
-    vt_status st = ensure_host(pages, hs, &disk);
-    if (st != VT_OK) { chunkFree_.push_back(c); return st; }
+    /* placement first (never-filled slots), so the chunk's own bricks count
+     * as apron sources for one another */
     C.pages = pages;
     C.slots.resize(n);
-    C.hslots = hs;
+    C.sources.clear();
     for (size_t i = 0; i < n; i++) {
         const int slot = freeSlots_.back();
         freeSlots_.pop_back();
@@ -1045,20 +1085,76 @@ vt_status BrickCache::spec_issue(const std::vector<uint64_t>& pages, int64_t* lo
         slotBrick_[slot] = pages[i];
         pageMirror_[p] = slot;
         stampHost_[slot] = pass_;
-        slotBusy_[slot] = 1;
-        hostBusy_[hs[i]] = 1;
+        slotBusy_[slot]++;
         specMark_[p] = 2;
         specChunkOf_[p] = c;
         C.slots[i] = slot;
-        SplitItem& it = C.hi[i];
-        it.hs = hs[i]; it.slot = slot; it.parts = kPartAll; it.staged = 0;
-        it.nb[0] = it.nb[1] = it.nb[2] = it.nb[3] = -1;
-        C.hu[i] = make_int2((int)p, slot);
     }
-    /* the bricks, then the page entries, after the data */
+    /* x/y aprons from neighbours resident now (not loading in another chunk)
+     * or placed in this chunk; a resident source stays busy -- no service
+     * evicts it -- until the chunk has landed */
+    const int Lc = cfg_.Lc;
+    const uint64_t grid = 1ull << Lc, msk = grid - 1;
+    const bool share = sharedAprons_ && cfg_.inc <= cfg_.edge;
+    std::vector<unsigned char> need(n, (unsigned char)kPartAll);
+    bool anyX = false, anyY = false;
+    for (size_t i = 0; i < n; i++) {
+        SplitItem& it = C.hi[i];
+        it.slot = C.slots[i]; it.parts = kPartAll; it.staged = 0;
+        it.nb[0] = it.nb[1] = it.nb[2] = it.nb[3] = -1;
+        if (!share) continue;
+        const uint64_t p = pages[i] - pageBase_;
+        const uint64_t bx = p >> (2 * Lc), by = (p >> Lc) & msk;
+        const bool inGrid[4] = {bx > 0, bx + 1 < grid, by > 0, by + 1 < grid};
+        const uint64_t nbPage[4] = {p - (1ull << (2 * Lc)), p + (1ull << (2 * Lc)), p - (1ull << Lc), p + (1ull << Lc)};
+        const unsigned char bit[4] = {kPartXm, kPartXp, kPartYm, kPartYp};
+        unsigned char parts = kPartM;
+        for (int d = 0; d < 4; d++) {
+            const int sl = inGrid[d] ? pageMirror_[nbPage[d]] : -1;
+            const bool ours = sl >= 0 && specMark_[nbPage[d]] == 2 && specChunkOf_[nbPage[d]] == c;
+            if (sl >= 0 && (ours || specMark_[nbPage[d]] != 2)) {
+                it.nb[d] = sl;
+                if (!ours) { slotBusy_[sl]++; C.sources.push_back(sl); }
+            } else {
+                parts |= bit[d];
+            }
+        }
+        anyX = anyX || it.nb[0] >= 0 || it.nb[1] >= 0;
+        anyY = anyY || it.nb[2] >= 0 || it.nb[3] >= 0;
+        need[i] = it.parts = parts;
+    }
+    std::vector<int> hs;
+    int64_t disk = 0;
+    vt_status st = ensure_host(pages, hs, &disk, 0, &need);
+    if (st != VT_OK) {
+        /* nothing of the chunk loads: its slots are never-filled again */
+        for (size_t i = 0; i < n; i++) {
+            const uint64_t p = pages[i] - pageBase_;
+            slotBrick_[C.slots[i]] = kEmpty;
+            pageMirror_[p] = -1;
+            slotBusy_[C.slots[i]]--;
+            specMark_[p] = 0;
+            specChunkOf_[p] = -1;
+            freeSlots_.push_back(C.slots[i]);
+        }
+        for (int sl : C.sources) slotBusy_[sl]--;
+        C.sources.clear();
+        chunkFree_.push_back(c);
+        return st;
+    }
+    C.hslots = hs;
+    for (size_t i = 0; i < n; i++) {
+        hostBusy_[hs[i]] = 1;
+        C.hi[i].hs = hs[i];
+        C.hu[i] = make_int2((int)(pages[i] - pageBase_), C.slots[i]);
+    }
+    /* the bricks, then the page entries, after the data -- and after any
+     * page reset of the last service (deferred demand bricks) */
+    CKC(cudaStreamWaitEvent(specStream_, svcEv_, 0));
     CKC(cudaMemcpyAsync(C.di, C.hi, n * sizeof(SplitItem), cudaMemcpyHostToDevice, specStream_));
-    st = launch_loads(C.di, n, 1, specStream_);
-    if (st != VT_OK) return st;
+    if ((st = launch_loads(C.di, n, 1, specStream_)) != VT_OK) return st;
+    if (anyY && (st = launch_loads(C.di, n, 2, specStream_)) != VT_OK) return st;
+    if (anyX && (st = launch_loads(C.di, n, 3, specStream_)) != VT_OK) return st;
     launches_++;
     CKC(cudaMemcpyAsync(C.du, C.hu, n * sizeof(int2), cudaMemcpyHostToDevice, specStream_));
     k_page_update<<<(unsigned int)((n + 255) / 256), 256, 0, specStream_>>>(d_page_, C.du, (int)n, d_stamp_, pass_);

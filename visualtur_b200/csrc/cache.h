@@ -43,6 +43,11 @@ struct CacheConfig {
     int deviceSlots = 0, hostSlots = 0, hostThreads = 0;
     bool asyncSpec = true;   /* lookahead bricks load on a side stream while passes run */
     bool sharedAprons = true;   /* demand loads copy x/y aprons from resident neighbours */
+    /* with side-stream loads: a service loads at most this many demand
+     * bricks itself while never-filled slots can take them all, and queues
+     * the rest on the side stream, which loads them while the next pass runs
+     * (0: no bound) */
+    int demandBatch = 0;
 };
 
 /* parts of a slot (bit masks; see above) */
@@ -118,6 +123,7 @@ public:
     vt_status spec_work(cudaEvent_t passDone, int64_t* loaded);
     void set_async_spec(bool on);
     void set_shared_aprons(bool on) { sharedAprons_ = on; }
+    void set_demand_batch(int n) { demandBatch_ = n > 0 ? n : 0; }
     /* pages predicted for the coming frames (already marked requested
      * speculatively on the device): queued ahead of the lookahead queue */
     void spec_hint(const unsigned int* pages, size_t n);
@@ -195,6 +201,11 @@ private:
     std::vector<uint64_t> hostTick_;
     std::vector<unsigned char> hostMask_;    /* host slot -> parts it holds */
     bool sharedAprons_ = true;
+    int demandBatch_ = 0;
+    /* recorded on the service stream after deferred demand pages were set
+     * to "requested speculatively"; side-stream page updates wait for it */
+    cudaEvent_t svcEv_ = nullptr;
+    int64_t deferred_ = 0;
     uint64_t tick_ = 0;
     /* transfer lists */
     struct Xfer {
@@ -219,6 +230,7 @@ private:
         cudaEvent_t ev = nullptr;
         std::vector<uint64_t> pages;
         std::vector<int> slots, hslots;
+        std::vector<int> sources;                 /* other slots the chunk's apron copies read */
         SplitItem* hi = nullptr; SplitItem* di = nullptr;   /* loads */
         int2* hu = nullptr; int2* du = nullptr;   /* page updates */
         size_t cap = 0;
@@ -236,7 +248,8 @@ private:
     std::vector<SpecChunk> chunks_;          /* ring of chunks (index = issue order % size) */
     std::vector<int> chunkFree_;             /* chunks not in flight */
     std::vector<int> chunkLive_;             /* chunks in flight, issue order */
-    std::vector<unsigned char> slotBusy_, hostBusy_;   /* device / host slot read or written in flight */
+    std::vector<unsigned short> slotBusy_;   /* device slot: side-stream chunks in flight that write or read it */
+    std::vector<unsigned char> hostBusy_;    /* host slot read by a side-stream chunk in flight */
     unsigned int pass_ = 0, frameStart_ = 1;
     bool allResident_ = false;
     /* stats */

@@ -361,6 +361,7 @@ extern "C" void vt_default_options(vt_options* o) {
     o->spec_async = 1;
     o->wavefront = 0;
     o->shared_aprons = 1;
+    o->demand_batch = 0;
 }
 
 static vt_status validate(const vt_params* p, const vt_octree* o, const vt_options* opt) {
@@ -384,6 +385,7 @@ static vt_status validate(const vt_params* p, const vt_octree* o, const vt_optio
         if (opt->max_suspended < 0 || opt->max_requests < 0 || opt->pool_per_ray < 0)
             return fail(VT_ERR_INVALID, "queue bounds must be >= 0 (0 = default)");
         if (opt->wavefront < 0 || opt->wavefront > 8) return fail(VT_ERR_INVALID, "wavefront rounds must be in 0..8");
+        if (opt->demand_batch < 0) return fail(VT_ERR_INVALID, "demand_batch must be >= 0");
         if (opt->record_trace && (opt->trace_level < 1 || opt->trace_level > p->octreeLevel || opt->trace_level > 8))
             return fail(VT_ERR_INVALID, "trace_level must be in 1..min(octreeLevel, 8)");
     }
@@ -417,7 +419,8 @@ static vt_status init_handle(vt_handle* h) {
         cc.deviceSlots = p.maxElementsCache; cc.hostSlots = p.maxElementsCache_CPU;
         cc.hostThreads = h->opt.host_threads;
         cc.asyncSpec = h->opt.spec_async != 0;
-    cc.sharedAprons = h->opt.shared_aprons != 0;
+        cc.sharedAprons = h->opt.shared_aprons != 0;
+        cc.demandBatch = h->opt.demand_batch;
         h->cache = new vtrt::BrickCache();
         if ((s = h->cache->init(cc)) != VT_OK) return s;
         if (h->opt.preload && (size_t)p.maxElementsCache >= h->leafBricks.size()) {
@@ -540,6 +543,7 @@ extern "C" vt_status vt_change_cache(vt_handle* h, int nE, const int cDim[3], in
     cc.deviceSlots = nE; cc.hostSlots = h->p.maxElementsCache_CPU; cc.hostThreads = h->opt.host_threads;
     cc.asyncSpec = h->opt.spec_async != 0;
     cc.sharedAprons = h->opt.shared_aprons != 0;
+    cc.demandBatch = h->opt.demand_batch;
     h->cache = new vtrt::BrickCache();
     if ((s = h->cache->init(cc)) != VT_OK) return s;
     if (h->opt.preload && (size_t)nE >= h->leafBricks.size() &&
@@ -950,6 +954,7 @@ extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
     o.spec_async = t->spec_async;
     o.wavefront = t->wavefront;
     o.shared_aprons = t->shared_aprons;
+    o.demand_batch = t->demand_batch;
     vt_status s = validate(&h->p, h->oct, &o);
     if (s != VT_OK) return s;
     if (o.lookahead < 0 || o.lookahead > 64 || o.pops < 1 || o.blocks_per_sm < 1 || o.blocks_per_sm > 32)
@@ -958,6 +963,7 @@ extern "C" vt_status vt_set_tuning(vt_handle* h, const vt_tuning* t) {
     if (h->cache) {
         h->cache->set_async_spec(o.spec_async != 0);
         h->cache->set_shared_aprons(o.shared_aprons != 0);
+        h->cache->set_demand_batch(o.demand_batch);
     }
     return VT_OK;
 }
@@ -972,6 +978,7 @@ extern "C" vt_status vt_get_tuning(vt_handle* h, vt_tuning* t) {
     t->spec_async = h->opt.spec_async;
     t->wavefront = h->opt.wavefront;
     t->shared_aprons = h->opt.shared_aprons;
+    t->demand_batch = h->opt.demand_batch;
     return VT_OK;
 }
 
