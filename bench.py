@@ -791,7 +791,7 @@ def make_launcher(wl, r, cfg, torch, dev, stream, batch, predictor=None, warm=Fa
 
 # (frames per launch, lookahead, absent-brick candidates a ray may set aside)
 PAGING_CANDIDATES = ((8, 2, 0), (4, 2, 0), (2, 2, 0), (1, 2, 0), (1, 0, 0),
-                     (8, 0, 0), (4, 0, 0), (2, 0, 0), (4, 1, 0),
+                     (16, 0, 0), (8, 0, 0), (4, 0, 0), (2, 0, 0), (4, 1, 0),
                      (4, 2, 4), (2, 2, 4), (4, 0, 4), (2, 0, 4), (1, 0, 4), (4, 0, 2))
 HINT_THRESHOLDS = (None, 0.25, 0.8)                             # besides 0.5; None = no hints
 DEMAND_BATCHES = (8192,)                                        # besides 0 = no bound
