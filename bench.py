@@ -191,6 +191,83 @@ def huge_page_array(shape, dtype, offset=0):
     return m, np.frombuffer(m, dtype, count=int(np.prod(shape)), offset=offset).reshape(shape)
 
 
+def _madvise_huge(addr, nbytes):
+    import ctypes
+    try:
+        ctypes.CDLL("libc.so.6").madvise(ctypes.c_void_p(addr), ctypes.c_size_t(nbytes), 14)   # MADV_HUGEPAGE
+    except (OSError, AttributeError, TypeError):
+        pass
+
+
+def shared_dir(nbytes):
+    """A directory with room for a file of `nbytes` (shared memory first)."""
+    for d in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            st = os.statvfs(d)
+        except OSError:
+            continue
+        if st.f_bavail * st.f_frsize >= nbytes + (2 << 30):
+            return d
+    return None
+
+
+def shared_host_array(dist, local_rank, name, shape, dtype, offset, produce):
+    """One host array for all ranks of the node: local rank 0 creates it
+    in a file (shared memory where there is room) and fills it with
+    `produce(array)`, the others map the same file read-only.  The file is
+    unlinked once every rank has mapped it, so its memory goes with the
+    last mapping, whatever way the processes end.  Returns (mmap, array)."""
+    import mmap
+    nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    size = offset + nbytes
+    path = None
+    if local_rank == 0:
+        d = shared_dir(size)
+        if d is None:
+            raise RuntimeError("no room for a shared %.1f GB volume in /dev/shm or %s" %
+                               (size / 1e9, tempfile.gettempdir()))
+        path = os.path.join(d, "vtbench_%s_%d_%s" % (name, os.getpid(), os.environ.get("MASTER_PORT", "0")))
+        with open(path, "wb") as f:
+            f.truncate(size)
+    paths = [path]
+    dist.broadcast_object_list(paths, src=0)
+    path = paths[0]
+    if local_rank == 0:
+        with open(path, "r+b") as f:
+            m = mmap.mmap(f.fileno(), size, flags=mmap.MAP_SHARED, prot=mmap.PROT_READ | mmap.PROT_WRITE)
+        arr = np.frombuffer(m, dtype, count=int(np.prod(shape)), offset=offset).reshape(shape)
+        _madvise_huge(arr.ctypes.data - offset, size)
+        produce(arr)
+    dist.barrier()
+    if local_rank != 0:
+        with open(path, "rb") as f:
+            m = mmap.mmap(f.fileno(), size, flags=mmap.MAP_SHARED, prot=mmap.PROT_READ)
+        arr = np.frombuffer(m, dtype, count=int(np.prod(shape)), offset=offset).reshape(shape)
+        _madvise_huge(arr.ctypes.data - offset, size)
+    dist.barrier()
+    if local_rank == 0:
+        os.unlink(path)
+    return m, arr
+
+
+def rank_host_bytes(cfg_bytes, shared_bytes, local_world):
+    """Pinned host-tier bytes for one of `local_world` ranks: the config's,
+    unless the node's memory (after the shared volume and a reserve) does
+    not hold that many tiers."""
+    if local_world <= 1:
+        return cfg_bytes
+    try:
+        with open("/proc/meminfo") as f:
+            total = int(next(l for l in f if l.startswith("MemTotal")).split()[1]) * 1024
+    except (OSError, StopIteration, ValueError):
+        return cfg_bytes
+    # a reserve for the system and 6 GB for each rank's own process
+    budget = (total - shared_bytes - (16 << 30) - local_world * (6 << 30)) // local_world
+    if budget < (1 << 30):
+        raise RuntimeError("host memory too small for %d ranks' brick tiers" % local_world)
+    return min(cfg_bytes, budget)
+
+
 def volume_offset(cfg):
     """Where the host volume starts relative to a cache line: brick boxes
     start `inc` voxels before a brick boundary (a multiple of 64 bytes of z
@@ -341,38 +418,73 @@ def step_views(cfg, step):
 class Workload:
     """Volume (device generated), octree (GPU builder) and renderer."""
 
-    def __init__(self, cfg, torch, device, workdir, need_renderer=True, mode="best", warm=False):
+    def __init__(self, cfg, torch, device, workdir, need_renderer=True, mode="best", warm=False, share=None):
+        """share: None (one process), or (dist, local_rank, local_world) of a
+        multi-rank job: the node's ranks then share one host volume (local
+        rank 0 generates it and the octree), each rank's pinned brick tier
+        fits the node's memory next to the others', and each rank's host
+        reads use its share of the cores."""
         import visualtur_b200 as vt
         self.vt, self.cfg = vt, cfg
         n = cfg["n"]
         u8 = cfg["gen"] == "fractal"
         self.esize = 1 if u8 else 4
         vdt = torch.uint8 if u8 else torch.float32
+        ndt = np.uint8 if u8 else np.float32
+        dist_, local_rank, local_world = share if share else (None, 0, 1)
+        vol_bytes = n * n * n * self.esize
+        self.host_bytes = rank_host_bytes(cfg.get("host_bytes", 0), vol_bytes if local_world > 1 else 0, local_world)
+        self.host_threads = 0 if local_world <= 1 else max(1, (os.cpu_count() or 1) // local_world)
         t0 = time.time()
-        dvol = torch.empty(n * n * n, dtype=vdt, device=device)
-        if cfg["gen"] == "sphere":
-            c = (n - 1) / 2.0
-            vt.generate_volume(vt.VT_GEN_SPHERE, cfg["seed"], (n, n, n), (c, c, c, 0.25), device_ptr=dvol.data_ptr())
-        elif u8:
-            vt.generate_volume(vt.VT_GEN_FRACTAL_U8, cfg["seed"], (n, n, n), cfg["spheres"], device_ptr=dvol.data_ptr())
-        else:
-            vt.generate_volume(vt.VT_GEN_BLOBS, cfg["seed"], (n, n, n), cfg["blobs"], device_ptr=dvol.data_ptr())
-        torch.cuda.synchronize()
-        t1 = time.time()
-        self.octree_path = os.path.join(workdir, "vol_%s.oct" % cfg["gen"])
-        vt.build_octree_device(dvol.data_ptr(), vt.VT_U8 if u8 else vt.VT_F32, (n, n, n), cfg["iso"],
-                               self.octree_path)
-        t2 = time.time()
+        times = [t0, t0, t0]
+        octree_name = "vol_%s.oct" % cfg["gen"]
+
+        def produce(arr):
+            """generate on this GPU, build the octree, copy to `arr`"""
+            dvol = torch.empty(n * n * n, dtype=vdt, device=device)
+            if cfg["gen"] == "sphere":
+                c = (n - 1) / 2.0
+                vt.generate_volume(vt.VT_GEN_SPHERE, cfg["seed"], (n, n, n), (c, c, c, 0.25),
+                                   device_ptr=dvol.data_ptr())
+            elif u8:
+                vt.generate_volume(vt.VT_GEN_FRACTAL_U8, cfg["seed"], (n, n, n), cfg["spheres"],
+                                   device_ptr=dvol.data_ptr())
+            else:
+                vt.generate_volume(vt.VT_GEN_BLOBS, cfg["seed"], (n, n, n), cfg["blobs"], device_ptr=dvol.data_ptr())
+            torch.cuda.synchronize()
+            times[0] = time.time()
+            vt.build_octree_device(dvol.data_ptr(), vt.VT_U8 if u8 else vt.VT_F32, (n, n, n), cfg["iso"],
+                                   self.octree_path)
+            times[1] = time.time()
+            torch.from_numpy(arr.reshape(-1)).copy_(dvol)
+            torch.cuda.synchronize()
+            del dvol
+            torch.cuda.empty_cache()
+            times[2] = time.time()
+
         # host copy of the volume: the out-of-core source and the CPU baseline's input
-        self._host_map, arr = huge_page_array((n * n * n,), np.uint8 if u8 else np.float32, volume_offset(cfg))
-        self.host = torch.from_numpy(arr)
-        self.host.copy_(dvol)
-        torch.cuda.synchronize()
-        del dvol
-        torch.cuda.empty_cache()
-        self.volume = self.host.numpy().reshape(n, n, n)
-        t3 = time.time()
-        log("setup: generate %.1fs octree %.1fs host copy %.1fs" % (t1 - t0, t2 - t1, t3 - t2))
+        if local_world <= 1:
+            self.octree_path = os.path.join(workdir, octree_name)
+            self._host_map, arr = huge_page_array((n * n * n,), ndt, volume_offset(cfg))
+            produce(arr)
+            octree_bytes = None
+        else:
+            # the octree file travels from local rank 0 as bytes
+            self.octree_path = os.path.join(workdir, octree_name)
+            self._host_map, arr = shared_host_array(dist_, local_rank, "vol", (n * n * n,), ndt, volume_offset(cfg),
+                                                    produce)
+            blob = [open(self.octree_path, "rb").read() if local_rank == 0 else None]
+            dist_.broadcast_object_list(blob, src=0)
+            if local_rank != 0:
+                with open(self.octree_path, "wb") as f:
+                    f.write(blob[0])
+            octree_bytes = len(blob[0])
+        self.volume = arr.reshape(n, n, n)
+        t1, t2, t3 = times
+        log("setup: generate %.1fs octree %.1fs host copy %.1fs%s" %
+            (t1 - t0, t2 - t1, t3 - t2, "" if octree_bytes is None else
+             " (volume shared by %d ranks, %d host threads and %.1f GB pinned tier each)" %
+             (local_world, self.host_threads, self.host_bytes / 2 ** 30)))
         self.r = None
         if need_renderer:
             self.fm = vt.FileManager.wrap(self.volume)
@@ -392,7 +504,7 @@ class Workload:
         D = edge + 2 * cfg["inc"]
         slot = (D ** 3 * self.esize + 15) // 16 * 16
         dev = cfg.get("dev_bytes", 0) // slot or 8 ** levelC
-        host = cfg.get("host_bytes", 0) // slot or 8 ** levelC
+        host = self.host_bytes // slot or 8 ** levelC
         self.slots = (dev, host, slot)
         return vt.make_params(W=cfg["W"], H=cfg["H"], octreeFile=None, hdf5File=None, octreeLevel=cfg["levelO"],
                               levelCubes=levelC, dimCube=edge, cubeInc=cfg["inc"], distance=cfg["dist"],
@@ -401,7 +513,7 @@ class Workload:
     def renderer(self, mode, warm=False, brick=None):
         """A renderer in `mode` (cold cache unless the workload is resident
         or `warm`: every needed brick preloaded, for steady-state profiles)."""
-        opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=0,
+        opt = self.vt.default_options(resident=self.cfg["resident"], record_hits=0, host_threads=self.host_threads,
                                       preload=1 if (self.cfg["resident"] or warm) else 0,
                                       shared_aprons=SHARED_APRONS, **MODES[mode]["opts"])
         return self.vt.visualTur(self.params(brick), opt, volume=self.fm, octree=self.oc)
@@ -918,7 +1030,9 @@ def run_ours(args, cfg, rank, world, torch, dist):
     torch.cuda.set_device(dev)
     work = tempfile.mkdtemp(prefix="vtbench_")
     M = MODES[args.mode]
-    wl = Workload(cfg, torch, dev, work, mode=args.mode, warm=args.warm)
+    local_world = int(os.environ.get("LOCAL_WORLD_SIZE", world))
+    share = (dist, int(os.environ.get("LOCAL_RANK", 0)), local_world) if (dist is not None and local_world > 1) else None
+    wl = Workload(cfg, torch, dev, work, mode=args.mode, warm=args.warm, share=share)
     stream = torch.cuda.Stream(device=dev)
     frame0 = replica_first_frame(rank, args.warmup, args.steps)
     batch = 1 if (cfg["resident"] or "views" in cfg) else M["batch"]
@@ -1051,6 +1165,7 @@ def run_ours(args, cfg, rank, world, torch, dist):
     if not cfg["resident"]:
         conf["shared_aprons"] = aprons_used
         conf["demand_batch"] = batch_used
+        conf["host_tier_bytes"] = wl.host_bytes
         if P is not None and "views" not in cfg:
             conf["hint_threshold"] = getattr(L, "thr", None)
     line = {
