@@ -37,7 +37,7 @@ typedef enum {
     VT_ERR_NOMEM = 5,        /* host or device allocation failed */
     VT_ERR_TIMEOUT = 6,      /* a bounded device wait or frame loop gave up */
     VT_ERR_STACK = 7,        /* a ray's traversal stack overflowed */
-    VT_ERR_UNSUPPORTED = 8,  /* valid request this build does not handle */
+    VT_ERR_UNSUPPORTED = 8,  /* valid request the library does not handle */
     VT_ERR_STATE = 9         /* call not valid in the handle's state */
 } vt_status;
 

@@ -1,6 +1,6 @@
 /*
  * h5lite.cpp -- HDF5 container support for volume files, written from the
- * published HDF5 file-format specification (no libhdf5 in this build).
+ * published HDF5 file-format specification (libhdf5 is not linked).
  *
  * The reference reads its volume with libhdf5: one 3-D dataset, hyperslab
  * reads converted to H5T_IEEE_F32LE (src/FileManager.cu:13-167), and
