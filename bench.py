@@ -942,6 +942,11 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
 
     thr0 = 0.5 if P is not None else None
     rows = [run(b, la, thr0, sk) for b, la, sk in PAGING_CANDIDATES]
+    # one run of a cold stretch varies by a few per cent: the three fastest
+    # run again and keep their better time
+    for r0 in sorted(rows, key=lambda x: x["ms"])[:3]:
+        again = run(r0["frames_per_launch"], r0["lookahead"], thr0, r0["skip"])
+        r0["ms"] = min(r0["ms"], again["ms"])
     best = min(rows, key=lambda x: x["ms"])
     if P is not None:
         rows += [run(best["frames_per_launch"], best["lookahead"], t, best["skip"]) for t in HINT_THRESHOLDS]
