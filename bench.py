@@ -777,6 +777,18 @@ def product_frame_rgba(vtm, r, cam, torch, dev, stream):
     return buf.cpu().numpy().reshape(-1, 4)
 
 
+def launch_split(start, frames, batch):
+    """The launches that render frames [start, start + frames) `batch` at a
+    time: (first frame, frames in it, frames in the next launch)."""
+    out = []
+    f, end = start, start + frames
+    while f < end:
+        n = min(batch, end - f)
+        out.append((f, n, min(batch, end - f - n)))
+        f += n
+    return out
+
+
 def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, label="timed", e2e=None):
     """Renders `warmup` then `steps` consecutive frames in launches of
     L.batch; returns device ms (CUDA events on the launching stream) and
@@ -803,13 +815,8 @@ def timed_frames(L, frame0, warmup, steps, dist, clocks=None, flush_l2=False, la
             if L.P is not None:
                 L.P.reset_hints()
         r.reset_stats()
-        launches = []
-        f = frame0 + warmup
-        while f < frame0 + warmup + steps:
-            n = min(L.batch, frame0 + warmup + steps - f)
-            nxt = min(L.batch, frame0 + warmup + steps - f - n)
-            launches.append((f, n, L.cams(f, n), L.cams(f + n, nxt)))
-            f += n
+        launches = [(f, n, L.cams(f, n), L.cams(f + n, nxt))
+                    for f, n, nxt in launch_split(frame0 + warmup, steps, L.batch)]
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in launches]
         per = []
         if e2e is not None:
@@ -931,12 +938,11 @@ def tune_paging(wl, cfg, torch, dev, stream, P, f0, frames=96):
         with torch.cuda.stream(stream):
             torch.cuda.synchronize()
             a.record(stream)
-            for f in range(s0, s0 + frames, b):
-                # the last launch holds the frames that are left, as in the
-                # timed run (a full one would charge larger batches for
-                # frames past the stretch)
-                n = min(b, s0 + frames - f)
-                L.launch(L.cams(f, n), L.cams(f + n, min(b, s0 + frames - f - n)), f)
+            # the last launch holds the frames that are left, as in the timed
+            # run (a full one would charge larger batches for frames past the
+            # stretch)
+            for f, n, nxt in launch_split(s0, frames, b):
+                L.launch(L.cams(f, n), L.cams(f + n, nxt), f)
             e.record(stream)
             torch.cuda.synchronize()
         ms = a.elapsed_time(e)

@@ -4,6 +4,8 @@ candidate is a setting the library accepts."""
 import os
 import sys
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
@@ -38,3 +40,15 @@ def test_views_paging_candidates_are_valid_settings():
     assert (2, 0) in bench.VIEWS_PAGING          # the mode's own setting stays a candidate
     for la, sk in bench.VIEWS_PAGING:
         assert 0 <= la <= 64 and 0 <= sk <= 4
+
+
+@pytest.mark.parametrize("frames,batch", [(20, 8), (20, 16), (20, 4), (300, 16), (7, 1), (3, 8)])
+def test_launch_split_covers_the_stretch_once(frames, batch):
+    """Timed runs and tuner trials render exactly the frames of their
+    stretch: the last launch holds only what is left (a trial that rendered
+    whole batches charged large batches for frames past the stretch)."""
+    out = bench.launch_split(40, frames, batch)
+    got = [f for f0, n, _ in out for f in range(f0, f0 + n)]
+    assert got == list(range(40, 40 + frames))
+    assert all(0 < n <= batch for _, n, _ in out)
+    assert [nxt for _, _, nxt in out] == [n for _, n, _ in out[1:]] + [0]
